@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark: forward+backward Sinkhorn iterations/s of the dictionary-learning
+objective (evaluate_both) on the batched 128x128 workload.
+
+One step = one evaluate_both over all P histograms of a rank: L forward Bregman
+iterations with the iterate store, the loss, and the reverse pass through the
+stored iterates for the atom and weight gradients.  Its unit of work is one
+histogram-iteration (P*L per step, all K atoms, forward and backward).
+
+Workload (per rank): P=64 seeded blob histograms (2-5 blobs) on 128x128, K=5
+atoms, L=100, gamma=1, KL loss.  Under torchrun each rank owns its own 64
+histograms (weak scaling); the dictionary gradient and the loss are summed
+across ranks with one NCCL all-reduce per step (the path's only exchange).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision split_bf16|tf32|fp32|fp64]
+    python bench.py --impl reference      # the reference's own CPU path (oracle/_ref)
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd Sinkhorn iters/s (128², K=5) vs plain FP32; p50/p99 serve latency"
+UNIT = "hist-iter/s"
+WORKLOAD = dict(name="batched128", P=64, W=128, H=128, K=5, L=100, gamma=1.0, loss=4,
+                n_blobs=(2, 5))
+CPU_SAMPLE_P = 4  # histograms in the bounded CPU sample (full L)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def default_precision():
+    return os.environ.get("WDL_BENCH_PRECISION", "fp32")
+
+
+def dtype_name(precision):
+    return {"fp32": "f32", "tf32": "tf32+f32", "split_bf16": "bf16x3+f32", "fp64": "f64"}[precision]
+
+
+# ---------------------------------------------------------------- CPU arms ---------
+def cpu_threads():
+    return len(os.sched_getaffinity(0))
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def time_cpu_reference(steps=1, warmup=0):
+    """The reference's own evaluate_both (GaussianSSE2DKernel, OpenMP over all
+    host cores) on a bounded sample: CPU_SAMPLE_P histograms at the full L."""
+    from oracle import oracle as orc
+    from wassersteindictionarylearning_b200.synthetic import make_problem, to_variables
+    w = WORKLOAD
+    P = CPU_SAMPLE_P
+    cfg, obs, atoms, wts = make_problem(None, seed=0, P=P, W=w["W"], H=w["H"], K=w["K"], L=w["L"],
+                                        gamma=w["gamma"], loss=w["loss"], n_blobs=w["n_blobs"])
+    x = to_variables(wts, atoms, cfg["scale_dic"])
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+    if orc.ref_available():
+        lib, kind = orc.RefLib(), "reference"
+
+        def run():
+            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], w["L"], w["loss"],
+                                     cfg["scale_dic"], x, obs, kind=1)
+        cores = lib.omp_threads()
+        what = "GaussianSSE2DKernel evaluate_both (cpp/inverseWasserstein.h:986), OpenMP"
+    else:
+        lib, kind = orc.OracleLib(), "port"
+        cores = cpu_threads()
+
+        def run():
+            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], w["L"], w["loss"],
+                                     cfg["scale_dic"], x, obs, nthreads=cores)
+        what = "C restatement evaluate_both, OpenMP over histograms"
+    for _ in range(warmup):
+        run()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    per_step = statistics.median(times)
+    units = P * w["L"]
+    return dict(value=units / per_step, unit=UNIT, cores=cores, kind=kind,
+                sample=f"{what}; {P} of 64 histograms at full size (128x128, K=5, L=100, KL), "
+                       f"{units} hist-iters per step, median of {steps}; CPU: {cpu_model()}"), per_step
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    base, per_step = time_cpu_reference(steps=args.steps, warmup=min(args.warmup, 1))
+    line = dict(metric=METRIC, value=base["value"], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=per_step * 1e3, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload=WORKLOAD["name"], P=CPU_SAMPLE_P, W=128, H=128, K=5, L=100,
+                            gamma=1.0, loss="KL", note="bounded sample of the batched workload"),
+                impl="reference", cpu_baseline=base,
+                e2e=dict(value=base["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks ------------
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        except OSError:
+            pass
+        finally:
+            if self.path:
+                os.unlink(self.path)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=mx,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+# ---------------------------------------------------------------- GPU arm -----------
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import wassersteindictionarylearning_b200 as w
+    from wassersteindictionarylearning_b200 import _lib
+    from wassersteindictionarylearning_b200.synthetic import make_problem, to_variables
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    precision = args.precision or default_precision()
+    wl = WORKLOAD
+    P, W, H, K, L = wl["P"], wl["W"], wl["H"], wl["K"], wl["L"]
+    N = W * H
+    cfg, obs, atoms, wts = make_problem(None, seed=1000 * rank, P=P, W=W, H=H, K=K, L=L,
+                                        gamma=wl["gamma"], loss=wl["loss"], n_blobs=wl["n_blobs"])
+    sd = cfg["scale_dic"]
+    x = to_variables(wts, atoms, sd)
+    n = x.size
+    PK = P * K
+    kern = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
+    ctx = kern.ctx
+    L_ = _lib.lib()
+    dev = torch.device("cuda", local)
+    x_d = torch.from_numpy(x).to(dev)
+    obs_d = torch.from_numpy(obs.reshape(-1)).to(dev)
+    g_d = torch.empty(n, dtype=torch.float64, device=dev)
+    f_d = torch.empty(1, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    fg = torch.empty(K * N + 1, dtype=torch.float64, device=dev)
+
+    def step():
+        rc = L_.wdl_evaluate_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(x_d.data_ptr()),
+                                         C.c_void_p(g_d.data_ptr()), n,
+                                         C.c_void_p(obs_d.data_ptr()), C.c_void_p(f_d.data_ptr()),
+                                         None, None, None, sptr)
+        _lib.check(rc, ctx)
+        if world > 1:  # the path's one exchange: dictionary gradient + loss
+            fg[: K * N].copy_(g_d[PK:])
+            fg[K * N:].copy_(f_d)
+            dist.all_reduce(fg)
+            g_d[PK:].copy_(fg[: K * N])
+            f_d.copy_(fg[K * N:])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    tape_gb = L_.wdl_eval_bytes(ctx, P, K, L) / 1e9
+
+    launches0 = L_.wdl_launch_count(ctx)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    gpu_launches = L_.wdl_launch_count(ctx) - launches0
+    clocks = clk.summary()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = P * L * args.steps * world
+    value = units / (ms / 1e3)
+    fval = float(f_d.item())
+
+    # Dominant kernel (the separable operator): average duration over one profiled
+    # step, with CUDA events on the launching stream, outside the timed loop.
+    L_.wdl_set_profiling(ctx, 1)
+    step()
+    torch.cuda.synchronize()
+    conv_ms, conv_launches, conv_imgs = C.c_double(), C.c_longlong(), C.c_double()
+    L_.wdl_conv_profile(ctx, C.byref(conv_ms), C.byref(conv_launches), C.byref(conv_imgs))
+    L_.wdl_set_profiling(ctx, 0)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    flop_per_img = 2.0 * N * (W + H)  # dense separable contraction, both axes
+    products = 3 if precision == "split_bf16" else 1
+    conv_launch_ms = conv_ms.value / max(conv_launches.value, 1)
+    imgs_per_launch = conv_imgs.value / max(conv_launches.value, 1)
+    achieved_tflops = flop_per_img * imgs_per_launch * products / (conv_launch_ms * 1e-3) / 1e12
+    if precision in ("split_bf16", "tf32"):
+        peak = peaks.get("bf16_tflops", 1590.0) * (0.5 if precision == "tf32" else 1.0)
+        peak_src = "of measured bf16 burst" if peaks else "of fallback"
+        bound = "tensor"
+    else:
+        # CUDA-core FMA peak: 148 SMs x 128 lanes x 2 flop x max SM clock (nominal)
+        mhz = peaks.get("sm_max_mhz", 1965.0)
+        peak = 148 * 128 * 2 * mhz * 1e6 / 1e12 / (2.0 if precision == "fp64" else 1.0)
+        peak_src = "of nominal CUDA-core FMA peak at max clock"
+        bound = "fp32-cuda-core" if precision == "fp32" else "fp64-cuda-core"
+    roofline = dict(bound=bound, achieved=achieved_tflops, peak=peak, unit="TFLOP/s",
+                    frac=achieved_tflops / peak, traffic=None, peak_source=peak_src,
+                    kernel="separable Gaussian operator (one launch = one operator application "
+                           f"over {imgs_per_launch:.0f} images)",
+                    conv_share_of_step=conv_ms.value / (ms / args.steps))
+
+    # End to end through the public host-pointer API (pinned host buffers).
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.from_numpy(x).pin_memory()
+        oh = torch.from_numpy(obs.reshape(-1)).pin_memory()
+        gh = torch.empty(n, dtype=torch.float64).pin_memory()
+        fh = torch.empty(1, dtype=torch.float64).pin_memory()
+        dp = C.POINTER(C.c_double)
+
+        def host_step():
+            rc = L_.wdl_evaluate_both(ctx, P, K, L, wl["loss"], sd,
+                                      C.cast(xh.data_ptr(), dp), C.cast(gh.data_ptr(), dp), n,
+                                      C.cast(oh.data_ptr(), dp), C.cast(fh.data_ptr(), dp),
+                                      None, None, None)
+            _lib.check(rc, ctx)
+            if world > 1:
+                fg[: K * N].copy_(gh[PK:].to(dev, non_blocking=False))
+                fg[K * N:] = float(fh[0])
+                dist.all_reduce(fg)
+                gh[PK:].copy_(fg[: K * N].cpu())
+        host_step()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            host_step()
+        el = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        h2d = (n + P * N) * 8 + (K * N * 8 if world > 1 else 0)
+        d2h = (n + 1) * 8 + (K * N * 8 if world > 1 else 0)
+        e2e = dict(value=units / el, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = time_cpu_reference(steps=1, warmup=0)
+
+    if world > 1:
+        torch.cuda.synchronize()
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+                warmup=args.warmup, ms_per_step=ms / args.steps, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype=dtype_name(precision),
+                data="synthetic: seeded anisotropic Gaussian-blob histograms (2-5 blobs), "
+                     "uniform+noise atoms, U[0,1] weights",
+                config=dict(workload="batched128: P=64 per GPU, 128x128, K=5, L=100, gamma=1, KL loss",
+                            P_per_gpu=P, W=W, H=H, K=K, L=L, gamma=wl["gamma"], loss="KL",
+                            precision=precision, parallelism=f"dp{world} over histograms",
+                            l2=f"working set larger than L2: iterate store {tape_gb:.2f} GB per GPU",
+                            objective=fval),
+                roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=int(gpu_launches),
+                clocks=clocks)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

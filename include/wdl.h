@@ -1,0 +1,163 @@
+/* wdl.h — C ABI of the B200 Sinkhorn-barycenter library (libwdl_b200.so).
+ *
+ * Drop-in boundary for the hot path of Wasserstein dictionary learning
+ * (reference: matthieuheitz/WassersteinDictionaryLearning, cpp/).  Everything
+ * below takes plain pointers and sizes; no exception crosses it; every call
+ * returns an int status (WDL_OK = 0, negative WDL_ERR_* on failure, described
+ * by wdl_strerror / wdl_last_error).  There is no CPU fallback: without a
+ * usable sm_100 device, wdl_create fails with WDL_ERR_NO_DEVICE.
+ *
+ * Data layout is the reference's: an image of N = W*H*D pixels is row-major
+ * with x fastest (index y*W + x, 3-D z*W*H + y*W + x); K images are stacked
+ * with stride N; P histograms are stacked with stride N; weights are [P][K];
+ * the L-BFGS vector is x = [P*K scaled log-weights, K*N log-atoms]
+ * (cpp/main_dictionary_learning.cpp:139-159, cpp/inverseWasserstein.h:389-401).
+ *
+ * Host-pointer calls copy in, run on the context's stream and copy out before
+ * returning.  *_device calls take device pointers and a cudaStream_t passed as
+ * void* (NULL = the context's stream) and return without synchronising.
+ * One host thread per context; a context is not safe for concurrent calls.
+ */
+#ifndef WDL_H
+#define WDL_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WDL_ABI_VERSION 1
+
+/* Status codes.  The reference has no error channel of its own (convolutions
+ * return void); its only codes are liblbfgs' (cpp/lbfgs/lbfgs.h:74-147), which
+ * wdl_lbfgs_* reuse with the same values. */
+enum {
+  WDL_OK = 0,
+  WDL_ERR_INVALID_ARG = -1,
+  WDL_ERR_CUDA = -2,
+  WDL_ERR_OUT_OF_MEMORY = -3,
+  WDL_ERR_UNSUPPORTED = -4,
+  WDL_ERR_NONFINITE = -5,   /* a loss or gradient came out NaN/Inf */
+  WDL_ERR_TIMEOUT = -6,     /* a bounded device or host wait gave up */
+  WDL_ERR_ADMISSION = -7,   /* serving: request larger than the HBM budget */
+  WDL_ERR_NO_DEVICE = -8,
+  WDL_ERR_BUSY = -9
+};
+
+/* Arithmetic of the separable convolutions.  FP32/TF32/SPLIT_BF16 keep the
+ * Sinkhorn scalings, tape and elementwise work in FP32 and reduce loss and
+ * gradients over grid and batch in FP64; FP64 runs everything in FP64 and
+ * keeps the reference's EPSILON = 1e-250 floor (cpp/kernels.h:30). */
+typedef enum {
+  WDL_FP32 = 0,        /* CUDA-core FP32 FMA                                   */
+  WDL_TF32 = 1,        /* tcgen05 kind::tf32, FP32 accumulate                  */
+  WDL_SPLIT_BF16 = 2,  /* tcgen05 kind::f16, hi+lo BF16, 3 products, FP32 acc  */
+  WDL_FP64 = 3         /* CUDA-core FP64                                       */
+} wdl_precision;
+
+typedef enum {
+  WDL_DOMAIN_KERNEL = 0, /* scalings as values (compute_gradient_both)              */
+  WDL_DOMAIN_LOG = 1     /* scalings as logs (compute_gradient_both_log_signArray)  */
+} wdl_domain;
+
+/* Loss indices follow the app's -l flag (cpp/main_dictionary_learning.cpp:189-197). */
+typedef enum {
+  WDL_LOSS_TV = 1,
+  WDL_LOSS_QUADRATIC = 2,
+  WDL_LOSS_WASSERSTEIN = 3,
+  WDL_LOSS_KL = 4
+} wdl_loss;
+
+typedef struct wdl_ctx wdl_ctx;
+
+/* Library and error strings. */
+int wdl_abi_version(void);
+const char* wdl_strerror(int status);
+/* Detail of the last failing call on ctx (or of the last failing wdl_create
+ * when ctx is NULL). */
+const char* wdl_last_error(const wdl_ctx* ctx);
+
+/* Context for one grid (W, H, D; D = 1 for 2-D) and regularisation gamma.
+ * Replaces a KernelType object's construction, e.g. Gaussian2DKernel(gamma, W, H)
+ * (cpp/kernels.h:632-641), Gaussian3DKernel (:714-725),
+ * LogSignArrayGaussian2DKernel (:1036-1045).  device < 0 selects the current device. */
+int wdl_create(wdl_ctx** ctx, int device, int W, int H, int D, double gamma, int precision,
+               int domain);
+int wdl_destroy(wdl_ctx* ctx);
+/* Waits for the context's stream. */
+int wdl_synchronize(wdl_ctx* ctx);
+/* Bytes of device memory a wdl_gradient_both / wdl_evaluate_both call with these
+ * sizes allocates (iterate store + workspace). */
+size_t wdl_eval_bytes(const wdl_ctx* ctx, int P, int K, int L);
+
+/* ---- KernelType operator (host pointers) ---------------------------------
+ * Gaussian2DKernel::convolve / convolveAdjoint (cpp/kernels.h:669-704),
+ * Gaussian3DKernel::convolve (:762-811): out_v = G (*) u_v for nvectors stacked
+ * images; the operator is symmetric, so the adjoint is the same call.  out may
+ * alias u. */
+int wdl_convolve(wdl_ctx* ctx, const double* u, double* out, int nvectors);
+/* LogSignArrayGaussian2DKernel::log_convolve (cpp/kernels.h:1073-1115). */
+int wdl_log_convolve(wdl_ctx* ctx, const double* log_u, double* out, int nvectors);
+/* log_convolve_signArray (cpp/kernels.h:1117-1163): signs (bit=1 means >= 0,
+ * bit i of byte i/8, cpp/signArray.h:8-22) are read for the input and
+ * overwritten with the output's signs. */
+int wdl_log_convolve_signed(wdl_ctx* ctx, const double* log_u, unsigned char* signs, double* out,
+                            int nvectors);
+
+/* ---- Hot path (host pointers) ------------------------------------------------
+ * compute_gradient_both / compute_gradient_both_log_signArray
+ * (cpp/inverseWasserstein.h:544-674, :678-814) for P histograms in one call:
+ * the device-resident replacement of the per-histogram loop of evaluate_both
+ * (:1052-1113).  atoms [K*N] and weights [P*K] are normalised first
+ * (Problem::normalize_values, :53-74).
+ *   result_la   [P*K]  raw weight gradient of each histogram (resultLa)
+ *   result_dic  [K*N]  raw dictionary gradient summed over the P histograms
+ *   bary        [P*N]  barycenters, or NULL
+ *   loss        [P]    loss of each barycenter against its observation, or NULL
+ *   b_init      [P*K*N] initial scalings b[0] (warm restart), or NULL for ones
+ *   b_last      [P*K*N] receives b[L] (warm restart store), or NULL */
+int wdl_gradient_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                      const double* weights, const double* observed, const double* b_init,
+                      double* result_la, double* result_dic, double* bary, double* loss,
+                      double* b_last);
+
+/* evaluate_both (cpp/inverseWasserstein.h:986-1145) with exp_weight = true:
+ * x[n] -> objective *f and gradient g[n], n = P*K + K*N.  b_storage / b_last as
+ * above (warm restart, :1057-1061, :1081-1085); bary [P*N] or NULL. */
+int wdl_evaluate_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                      const double* x, double* g, int n, const double* observed, double* f,
+                      const double* b_storage, double* b_last, double* bary);
+
+/* WassersteinBarycenter::compute_barycenter / _log (cpp/inverseWasserstein.h:115-201):
+ * forward Bregman projections only, for P weight vectors against one set of atoms.
+ * bary [P*N]. */
+int wdl_barycenter(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
+                   double* bary);
+
+/* ---- Device-resident forms (device pointers, stream as void*) ----------------
+ * Same semantics as the host forms; no host<->device copies, no synchronisation.
+ * f is a device double. */
+int wdl_evaluate_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                             const double* x, double* g, int n, const double* observed, double* f,
+                             const double* b_storage, double* b_last, double* bary, void* stream);
+int wdl_gradient_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                             const double* weights, const double* observed, const double* b_init,
+                             double* result_la, double* result_dic, double* bary, double* loss,
+                             double* b_last, void* stream);
+int wdl_convolve_device(wdl_ctx* ctx, const double* u, double* out, int nvectors, void* stream);
+
+/* ---- Instrumentation ------------------------------------------------------------
+ * Kernel launches issued by this context since creation (every kernel of this
+ * library counts one), and the last call's time in the dominant convolution
+ * kernel as measured with CUDA events on the launching stream (0 unless
+ * wdl_set_profiling(ctx, 1)). */
+long long wdl_launch_count(const wdl_ctx* ctx);
+int wdl_set_profiling(wdl_ctx* ctx, int on);
+int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launches,
+                     double* conv_images);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WDL_H */

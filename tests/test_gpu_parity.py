@@ -1,0 +1,204 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden
+outputs and the oracle.
+
+Tolerances (normwise relative error ||x - ref||_inf / ||ref||_inf against the
+FP64 reference):
+  FP64 mode   1e-10 for every output
+  FP32 mode   1e-5  for barycenters, losses, gradients
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32": 1e-5}
+
+
+def kern(gamma, W, H, D=1, precision="fp64", log=False):
+    from wassersteindictionarylearning_b200 import (CudaGaussian2DKernel, CudaGaussian3DKernel,
+                                                     CudaLogSignArrayGaussian2DKernel)
+    if log:
+        return CudaLogSignArrayGaussian2DKernel(gamma, W, H, precision=precision)
+    if D > 1:
+        return CudaGaussian3DKernel(gamma, W, H, D, precision=precision)
+    return CudaGaussian2DKernel(gamma, W, H, precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("conv_*"))
+def test_convolve(name, f, precision):
+    k = kern(float(f["gamma"]), int(f["W"]), int(f["H"]), int(f["D"]), precision)
+    out = k.convolve(f["u"], int(f["nv"]))
+    assert rel(out, f["out"]) < (1e-13 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("logconv_*"))
+def test_log_convolve(name, f, precision):
+    W, H, nv = int(f["W"]), int(f["H"]), int(f["nv"])
+    k = kern(float(f["gamma"]), W, H, precision=precision, log=True)
+    tol = 1e-13 if precision == "fp64" else 1e-5
+    assert rel(k.log_convolve(f["u"], nv), f["out"]) < tol
+    signs = f["signs_in"].copy()
+    out = k.log_convolve_signArray(f["u"], signs, nv)
+    if precision == "fp64":
+        assert np.array_equal(signs, f["signs_out"])
+        assert rel(out, f["out_signed"]) < tol
+    else:  # near-cancelling sums may flip; compare where the reference is far from 0
+        ok = np.unpackbits(signs, bitorder="little")[: W * H * nv] == \
+            np.unpackbits(f["signs_out"], bitorder="little")[: W * H * nv]
+        assert ok.mean() > 0.97
+
+
+def _regression(W, H, D, gamma, P, K, L, loss, sd, obs, precision, log=False):
+    from wassersteindictionarylearning_b200 import Problem, WassersteinRegression
+    k = kern(gamma, W, H, D, precision, log)
+    prob = Problem(np.ones((K, W * H * D)), obs, k, None, P)
+    return WassersteinRegression(prob, L, loss, sd)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("grad_*"))
+def test_gradient_both(name, f, precision):
+    W, H, D, K, L = int(f["W"]), int(f["H"]), int(f["D"]), int(f["K"]), int(f["L"])
+    reg = _regression(W, H, D, float(f["gamma"]), 1, K, L, int(f["loss"]), 1.0, f["obs"], precision)
+    la, dic, bary, _ = reg.compute_gradient_both(f["atoms"], f["lambdas"])
+    tol = TOL[precision]
+    assert rel(bary, f["bary"]) < tol
+    assert rel(dic, f["resultDic"]) < tol
+    assert rel(la, f["resultLa"]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("gradlog_*"))
+def test_gradient_both_log(name, f, precision):
+    W, H, K, L = int(f["W"]), int(f["H"]), int(f["K"]), int(f["L"])
+    reg = _regression(W, H, 1, float(f["gamma"]), 1, K, L, int(f["loss"]), 1.0, f["obs"], precision,
+                      log=True)
+    la, dic, bary, _ = reg.compute_gradient_both(f["atoms"], f["lambdas"])
+    tol = TOL[precision]
+    assert rel(bary, f["bary"]) < tol
+    assert rel(dic, f["resultDic"]) < tol
+    assert rel(la, f["resultLa"]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("bary_*"))
+def test_barycenter(name, f, precision):
+    from wassersteindictionarylearning_b200 import Problem, WassersteinBarycenter
+    W, H, D, K, L = int(f["W"]), int(f["H"]), int(f["D"]), int(f["K"]), int(f["L"])
+    k = kern(float(f["gamma"]), W, H, D, precision, log=bool(f["log"]))
+    prob = Problem(f["atoms"], np.zeros(W * H * D), k, f["lambdas"], 1)
+    b = WassersteinBarycenter(prob, L).compute_barycenter()
+    assert rel(b, f["bary"]) < TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,f", golden("eval_*"))
+def test_evaluate_both(name, f, precision):
+    W, H, D, P, K, L = (int(f[k]) for k in ("W", "H", "D", "P", "K", "L"))
+    reg = _regression(W, H, D, float(f["gamma"]), P, K, L, int(f["loss"]), float(f["scale_dic"]),
+                      f["obs"], precision, log=bool(f["log"]))
+    fv, g = reg.evaluate_both(f["x"])
+    tol = TOL[precision]
+    assert abs(fv - float(f["f"])) <= tol * abs(float(f["f"]))
+    assert rel(g, f["g"]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_warm_restart(precision):
+    (_, f), = golden("warm_*")
+    W, H, P, K, L = (int(f[k]) for k in ("W", "H", "P", "K", "L"))
+    reg = _regression(W, H, 1, float(f["gamma"]), P, K, L, int(f["loss"]), float(f["scale_dic"]),
+                      f["obs"], precision)
+    reg.warmRestart = True
+    reg.b_storage = f["b_storage"].copy()
+    fv, g = reg.evaluate_both(f["x"])
+    tol = TOL[precision]
+    assert abs(fv - float(f["f"])) <= tol * abs(float(f["f"]))
+    assert rel(g, f["g"]) < tol
+    assert rel(reg.b_temp, f["b_last"]) < tol
+
+
+def test_regress_both_matches_reference():
+    """Four L-BFGS iterations end to end through the GPU (FP64) land where the
+    reference's regress_both does."""
+    (_, f), = golden("regress_*")
+    W, H, P, K, L = (int(f[k]) for k in ("W", "H", "P", "K", "L"))
+    reg = _regression(W, H, 1, float(f["gamma"]), P, K, L, int(f["loss"]), float(f["scale_dic"]),
+                      f["obs"], "fp64")
+    reg.wrTotalIteration = int(f["iters"])
+    sol = f["solution0"].copy()
+    reg.regress_both(sol)
+    assert rel(sol, f["solution"]) < 1e-8
+
+
+# ---- larger cases against the oracle -----------------------------------------------
+def _problem(P, W, H, K, L, gamma, loss, D=1, seed=0, n_blobs=(1, 3)):
+    from wassersteindictionarylearning_b200.synthetic import make_problem, to_variables
+    cfg, obs, atoms, w = make_problem(None, seed=seed, P=P, W=W, H=H, D=D, K=K, L=L, gamma=gamma,
+                                      loss=loss, n_blobs=n_blobs)
+    x = to_variables(w, atoms, cfg["scale_dic"])
+    return cfg, obs, x
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("case", [
+    dict(P=16, W=64, H=64, K=4, L=25, gamma=2.0, loss=2),            # dictionary-learning shape
+    dict(P=4, W=128, H=128, K=5, L=20, gamma=1.0, loss=4, n_blobs=(2, 5)),  # batched shape, short L
+    dict(P=3, W=72, H=40, K=3, L=10, gamma=2.0, loss=1),             # ragged, non-square
+    dict(P=2, W=24, H=20, D=12, K=2, L=6, gamma=2.0, loss=2),        # 3-D
+])
+def test_evaluate_vs_oracle(oracle, case, precision):
+    case = dict(case)
+    D = case.pop("D", 1)
+    cfg, obs, x = _problem(D=D, **case)
+    W, H, P, K, L = cfg["W"], cfg["H"], cfg["P"], cfg["K"], cfg["L"]
+    f_ref, g_ref = oracle.evaluate_both(W, H, D, cfg["gamma"], P, K, L, cfg["loss"], cfg["scale_dic"],
+                                        x, obs)
+    reg = _regression(W, H, D, cfg["gamma"], P, K, L, cfg["loss"], cfg["scale_dic"], obs, precision)
+    fv, g = reg.evaluate_both(x)
+    tol = TOL[precision]
+    assert abs(fv - f_ref) <= tol * abs(f_ref)
+    PK = P * K
+    assert rel(g[:PK], g_ref[:PK]) < tol
+    assert rel(g[PK:], g_ref[PK:]) < tol
+
+
+def test_batch_invariance_and_determinism():
+    """Each histogram's outputs are the same alone and inside the batch; two
+    runs are bit-identical (no atomics in any reduction)."""
+    cfg, obs, x = _problem(P=6, W=48, H=40, K=3, L=12, gamma=2.0, loss=2)
+    W, H, P, K, L = cfg["W"], cfg["H"], cfg["P"], cfg["K"], cfg["L"]
+    from wassersteindictionarylearning_b200.synthetic import init_atoms, init_weights
+    atoms = init_atoms(K, W * H, seed=7)
+    w = init_weights(P, K, seed=8)
+    reg = _regression(W, H, 1, cfg["gamma"], P, K, L, cfg["loss"], 1.0, obs, "fp32")
+    la, dic, bary, loss = reg.compute_gradient_both(atoms, w)
+    la2, dic2, bary2, loss2 = reg.compute_gradient_both(atoms, w)
+    assert np.array_equal(la, la2) and np.array_equal(dic, dic2) and np.array_equal(bary, bary2)
+    for p in (0, 3, 5):
+        one = _regression(W, H, 1, cfg["gamma"], 1, K, L, cfg["loss"], 1.0, obs[p], "fp32")
+        la1, dic1, bary1, loss1 = one.compute_gradient_both(atoms, w[p])
+        assert np.array_equal(bary1, bary[p * W * H:(p + 1) * W * H])
+        assert np.array_equal(la1, la[p * K:(p + 1) * K])
+        assert loss1[0] == loss[p]
+
+
+def test_edge_cases():
+    from wassersteindictionarylearning_b200 import WdlError, _lib
+    import ctypes as C
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.wdl_create(C.byref(h), -1, 0, 8, 1, 1.0, 0, 0) == -1      # empty grid
+    assert L.wdl_create(C.byref(h), -1, 8, 8, 1, -1.0, 0, 0) == -1     # bad gamma
+    assert L.wdl_create(C.byref(h), -1, 8, 8, 2, 1.0, 0, 1) == -4      # 3-D log domain
+    k = kern(2.0, 1, 1)                                                # 1x1 grid
+    assert np.allclose(k.convolve(np.array([3.0])), [3.0])
+    k = kern(2.0, 8, 8)
+    assert k.convolve(np.zeros(0), 0).size == 0                        # zero images
+    with pytest.raises(WdlError):
+        _regression(8, 8, 1, 2.0, 1, 2, 3, 7, 1.0, np.ones(64) / 64, "fp32").compute_gradient_both(
+            np.ones(128), np.ones(2))                                  # unknown loss

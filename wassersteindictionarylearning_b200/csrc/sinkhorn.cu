@@ -1,0 +1,752 @@
+// Device-resident Sinkhorn-barycenter forward pass, loss, and reverse pass
+// through the stored iterates, for P histograms at once.
+//
+// This is the batched replacement of the per-histogram loop of evaluate_both
+// (cpp/inverseWasserstein.h:1052-1113) around compute_gradient_both (:544-674)
+// and compute_gradient_both_log_signArray (:678-814).  Histograms are laid out
+// [P][K][N] (histogram, atom, pixel) so that one launch of the separable
+// operator covers every histogram and atom of a step.  The dictionary and
+// weight recursions of the reverse pass are independent of each other (the
+// reference runs them one after the other); here they advance together, one
+// step s per round, so each round's two operator applications cover 2*P*K images
+// in one launch.  Elementwise work between operator applications is fused into
+// one kernel per round; every reduction over the grid or the batch (loss,
+// weight-gradient dot products, the sum of the dictionary gradient over P) runs
+// in FP64.
+#include <cmath>
+
+#include "wdl_internal.cuh"
+
+namespace wdl {
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T d_exp(T x);
+template <>
+__device__ __forceinline__ float d_exp<float>(float x) { return expf(x); }
+template <>
+__device__ __forceinline__ double d_exp<double>(double x) { return exp(x); }
+template <typename T>
+__device__ __forceinline__ T d_log(T x);
+template <>
+__device__ __forceinline__ float d_log<float>(float x) { return logf(x); }
+template <>
+__device__ __forceinline__ double d_log<double>(double x) { return log(x); }
+
+// safe_log = log(max(EPSILON, x)) (cpp/loss.h:3-5).
+template <typename T>
+__device__ __forceinline__ T safe_log(T x);
+template <>
+__device__ __forceinline__ double safe_log<double>(double x) {
+  return log(x > kEpsilon ? x : kEpsilon);
+}
+template <>
+__device__ __forceinline__ float safe_log<float>(float x) {
+  return x > 0.f ? logf(x) : float(kLogEpsilon);
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < nw ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+#define GRID_STRIDE(i, n) \
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
+template <typename T>
+__global__ void k_cast(const double* __restrict__ in, T* __restrict__ out, size_t n) {
+  GRID_STRIDE(i, n) out[i] = (T)in[i];
+}
+template <typename T>
+__global__ void k_cast_back(const T* __restrict__ in, double* __restrict__ out, size_t n) {
+  GRID_STRIDE(i, n) out[i] = (double)in[i];
+}
+template <typename T>
+__global__ void k_fill(T* __restrict__ p, T v, size_t n) {
+  GRID_STRIDE(i, n) p[i] = v;
+}
+template <typename T>
+__global__ void k_log_of(const double* __restrict__ in, T* __restrict__ out, size_t n) {
+  GRID_STRIDE(i, n) out[i] = (T)log(in[i]);
+}
+
+// Problem::normalize_values (cpp/inverseWasserstein.h:53-74), one row per block.
+// With exp_scale != 0 the row is first mapped through exp(v / exp_scale)
+// (evaluate_both's return to the original domain, :997-1011).
+__global__ void k_normalise_rows(const double* __restrict__ in, double* __restrict__ out,
+                                 size_t len, double exp_scale) {
+  __shared__ double sh[32];
+  const double* r = in + (size_t)blockIdx.x * len;
+  double* o = out + (size_t)blockIdx.x * len;
+  double s = 0;
+  for (size_t j = threadIdx.x; j < len; j += blockDim.x) {
+    double v = exp_scale != 0.0 ? exp(r[j] / exp_scale) : r[j];
+    o[j] = v;
+    s += v;
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) sh[0] = s;
+  __syncthreads();
+  s = sh[0];
+  for (size_t j = threadIdx.x; j < len; j += blockDim.x) o[j] = o[j] / s;
+}
+
+// ---------------- kernel-domain forward (cpp/inverseWasserstein.h:565-593) -----------
+// a = p / conv_b, the atoms shared by every histogram.
+template <typename T>
+__global__ void k_div_atoms(const T* __restrict__ atoms, const T* __restrict__ cb,
+                            T* __restrict__ a, size_t KN, size_t total) {
+  GRID_STRIDE(i, total) a[i] = atoms[i % KN] / cb[i];
+}
+
+// Weighted geometric mean over the K atoms and the next scalings b = bary / phi.
+template <typename T>
+__global__ void k_bary_b(const T* __restrict__ phi, const T* __restrict__ lam, T* __restrict__ b,
+                         T* __restrict__ bary, int K, size_t N, size_t PN) {
+  GRID_STRIDE(idx, PN) {
+    const size_t p = idx / N, j = idx - p * N;
+    const T* ph = phi + p * K * N + j;
+    T s = T(0);
+    for (int k = 0; k < K; ++k) s += safe_log<T>(ph[k * N]) * lam[p * K + k];
+    const T by = d_exp<T>(s);
+    bary[idx] = by;
+    if (b)
+      for (int k = 0; k < K; ++k) b[p * K * N + k * N + j] = by / ph[k * N];
+  }
+}
+
+// ---------------- log-domain forward (:700-720, :167-196) ---------------------------
+template <typename T>
+__global__ void k_log_sub_atoms(const T* __restrict__ log_atoms, const T* __restrict__ cb,
+                                T* __restrict__ a, size_t KN, size_t total) {
+  GRID_STRIDE(i, total) a[i] = log_atoms[i % KN] - cb[i];
+}
+
+template <typename T>
+__global__ void k_log_bary_b(const T* __restrict__ phi, const T* __restrict__ lam,
+                             T* __restrict__ b, T* __restrict__ bary_log, int K, size_t N,
+                             size_t PN) {
+  GRID_STRIDE(idx, PN) {
+    const size_t p = idx / N, j = idx - p * N;
+    const T* ph = phi + p * K * N + j;
+    T s = T(0);
+    for (int k = 0; k < K; ++k) s += ph[k * N] * lam[p * K + k];
+    bary_log[idx] = s;
+    if (b)
+      for (int k = 0; k < K; ++k) b[p * K * N + k * N + j] = s - ph[k * N];
+  }
+}
+
+template <typename T>
+__global__ void k_exp_inplace(T* __restrict__ v, size_t n) {
+  GRID_STRIDE(i, n) v[i] = d_exp<T>(v[i]);
+}
+
+// ---------------- loss (cpp/loss.h:19-90), one histogram per block ------------------
+// Writes the loss gradient g into n (the dictionary recursion's start) and
+// g * bary into gw (the weight recursion's start, :633-635).
+template <typename T>
+__global__ void k_loss(const T* __restrict__ bary, const double* __restrict__ obs,
+                       const T* __restrict__ wgrad, T* __restrict__ n, T* __restrict__ gw,
+                       double* __restrict__ loss, int loss_type, size_t N) {
+  __shared__ double sh[32];
+  const size_t p = blockIdx.x;
+  double acc = 0;
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+    const size_t i = p * N + j;
+    const T v1 = bary[i];
+    const double o = obs[i];
+    const T v2 = (T)o;
+    T g;
+    if (loss_type == WDL_LOSS_TV) {
+      const T d = v1 - v2;
+      acc += fabs((double)v1 - o);
+      g = d > T(0) ? T(0.5) : T(-0.5);
+    } else if (loss_type == WDL_LOSS_QUADRATIC) {
+      const double d = (double)v1 - o;
+      acc += d * d;
+      g = T(2) * (v1 - v2);
+    } else if (loss_type == WDL_LOSS_KL) {
+      const double r = (double)v1 / o;
+      acc += (double)v1 * log(r > kEpsilon ? r : kEpsilon) - (double)v1 + o;
+      g = safe_log<T>(v1 / v2);
+    } else {  // Wasserstein: gradient precomputed by the nested Sinkhorn
+      g = wgrad[i];
+    }
+    n[i] = g;
+    gw[i] = g * v1;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0 && loss_type != WDL_LOSS_WASSERSTEIN)
+    loss[p] = loss_type == WDL_LOSS_TV ? 0.5 * acc : acc;
+}
+
+// Wasserstein loss helpers (cpp/loss.h:92-154): a = v1 / Kb, b = v2 / Ka.
+template <typename T>
+__global__ void k_ratio(const T* __restrict__ num, const double* __restrict__ num64,
+                        const T* __restrict__ den, T* __restrict__ out, size_t n) {
+  GRID_STRIDE(i, n) out[i] = (num ? num[i] : (T)num64[i]) / den[i];
+}
+template <typename T>
+__global__ void k_wloss(const T* __restrict__ v1, const double* __restrict__ v2,
+                        const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ c,
+                        T* __restrict__ wgrad, double* __restrict__ loss, double gamma, size_t N) {
+  __shared__ double sh[32];
+  const size_t p = blockIdx.x;
+  double acc = 0;
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+    const size_t i = p * N + j;
+    const double la = (double)safe_log<T>(a[i]), lb = (double)safe_log<T>(b[i]);
+    acc += la * (double)v1[i] + lb * v2[i] - (double)a[i] * (double)c[i];
+    wgrad[i] = (T)(gamma * la);
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) loss[p] = gamma * acc;
+}
+
+// ---------------- kernel-domain reverse pass (:602-673), one round s ----------------
+// Block per (p, k): dictionary tmp = (lambda n - v) * b[s]; weights
+// dot += sum_j log(phi[s]) gw (plain log, as :649), u = (lambda gw - r) / phi[s].
+template <typename T>
+__global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
+                          const T* __restrict__ b_s, const T* __restrict__ gw,
+                          const T* __restrict__ r, const T* __restrict__ phi_s,
+                          const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u,
+                          double* __restrict__ dot, int K, size_t N) {
+  __shared__ double sh[32];
+  const size_t pk = blockIdx.x, p = pk / K;
+  const T l = lam[pk];
+  const size_t base = pk * N, pb = p * N;
+  double acc = 0;
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+    const size_t i = base + j;
+    tmp[i] = (l * n[pb + j] - v[i]) * b_s[i];
+    const T ph = phi_s[i];
+    const T g = gw[pb + j];
+    acc += (double)d_log<T>(ph) * (double)g;
+    u[i] = (l * g - r[i]) / ph;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) dot[pk] += acc;
+}
+
+// gradDic += c / cb[s-1]; tmp = -p c / cb^2; convu *= -p / cb^2 (:612-617, :655-660).
+template <typename T>
+__global__ void k_bwd_mid(const T* __restrict__ c, const T* __restrict__ cb,
+                          const T* __restrict__ atoms, double* __restrict__ gdic,
+                          T* __restrict__ nxt, size_t KN, size_t PKN, int weights) {
+  GRID_STRIDE(i, PKN) {
+    const T cbv = cb[i], cc = c[i], pa = atoms[i % KN];
+    gdic[i] += (double)(cc / cbv);
+    nxt[i] = -pa * cc / (cbv * cbv);
+    if (weights) nxt[PKN + i] = c[PKN + i] * (-pa / (cbv * cbv));
+  }
+}
+
+// v = Kt(tmp) / phi[s-1], n = sum_k v (:619-627); r = K(convu) * b[s-1],
+// gw = sum_k r (:661-669).  One thread per (p, pixel).
+template <typename T>
+__global__ void k_bwd_post(const T* __restrict__ c2, const T* __restrict__ phi_p,
+                           const T* __restrict__ b_p, T* __restrict__ v, T* __restrict__ r,
+                           T* __restrict__ n, T* __restrict__ gw, int K, size_t N, size_t PN,
+                           size_t PKN) {
+  GRID_STRIDE(idx, PN) {
+    const size_t p = idx / N, j = idx - p * N;
+    T sn = T(0), sg = T(0);
+    for (int k = 0; k < K; ++k) {
+      const size_t i = (p * K + k) * N + j;
+      const T vv = c2[i] / phi_p[i];
+      v[i] = vv;
+      sn += vv;
+      const T rr = c2[PKN + i] * b_p[i];
+      r[i] = rr;
+      sg += rr;
+    }
+    n[idx] = sn;
+    gw[idx] = sg;
+  }
+}
+
+// ---------------- log-domain reverse pass (:722-812), one round s -------------------
+// Signed quantities are (log|x|, sign byte) pairs; sd and sw are the dictionary
+// and weight recursions' sign arrays (cpp/signArray.h:24-35).
+template <typename T>
+__global__ void k_lbwd_pre(const T* __restrict__ n, const T* __restrict__ v,
+                           const T* __restrict__ b_s, const T* __restrict__ gw,
+                           const T* __restrict__ r, const T* __restrict__ phi_s,
+                           const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u,
+                           uint8_t* __restrict__ sd, uint8_t* __restrict__ sw,
+                           double* __restrict__ dot, int K, size_t N) {
+  __shared__ double sh[32];
+  const size_t pk = blockIdx.x, p = pk / K;
+  const T l = lam[pk];
+  const size_t base = pk * N, pb = p * N;
+  double acc = 0;
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+    const size_t i = base + j;
+    const T x = l * n[pb + j] + v[i];
+    sd[i] = x >= T(0);
+    tmp[i] = d_log<T>(fabs(x)) + b_s[i];
+    const T ph = phi_s[i];
+    const T g = gw[pb + j];
+    acc += (double)ph * (double)g;
+    const T y = l * g + r[i];
+    sw[i] = y >= T(0);
+    u[i] = d_log<T>(fabs(y)) - ph;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) dot[pk] += acc;
+}
+
+template <typename T>
+__global__ void k_lbwd_mid(const T* __restrict__ c, const T* __restrict__ cb,
+                           const T* __restrict__ log_atoms, const uint8_t* __restrict__ sd,
+                           double* __restrict__ gdic, T* __restrict__ nxt, size_t KN, size_t PKN,
+                           int weights) {
+  GRID_STRIDE(i, PKN) {
+    const T cbv = cb[i], cc = c[i], lp = log_atoms[i % KN];
+    const T e = d_exp<T>(cc - cbv);
+    gdic[i] += (double)(sd[i] ? e : -e);
+    nxt[i] = lp + cc - T(2) * cbv;
+    if (weights) nxt[PKN + i] = c[PKN + i] + (lp - T(2) * cbv);
+  }
+}
+
+template <typename T>
+__global__ void k_lbwd_post(const T* __restrict__ c2, const T* __restrict__ phi_p,
+                            const T* __restrict__ b_p, const uint8_t* __restrict__ sd,
+                            const uint8_t* __restrict__ sw, T* __restrict__ v,
+                            T* __restrict__ r, T* __restrict__ n, T* __restrict__ gw, int K,
+                            size_t N, size_t PN, size_t PKN) {
+  GRID_STRIDE(idx, PN) {
+    const size_t p = idx / N, j = idx - p * N;
+    T sn = T(0), sg = T(0);
+    for (int k = 0; k < K; ++k) {
+      const size_t i = (p * K + k) * N + j;
+      T e = d_exp<T>(c2[i] - phi_p[i]);
+      const T vv = sd[i] ? e : -e;
+      v[i] = vv;
+      sn -= vv;
+      e = d_exp<T>(c2[PKN + i] + b_p[i]);
+      const T rr = sw[i] ? e : -e;
+      r[i] = rr;
+      sg -= rr;
+    }
+    n[idx] = sn;
+    gw[idx] = sg;
+  }
+}
+
+// ---------------- reductions and evaluate_both epilogue (:1086-1136) ----------------
+__global__ void k_sum_over_p(const double* __restrict__ gdic, double* __restrict__ out, int P,
+                             size_t KN) {
+  GRID_STRIDE(i, KN) {
+    double s = 0;
+    for (int p = 0; p < P; ++p) s += gdic[(size_t)p * KN + i];
+    out[i] = s;
+  }
+}
+
+// Weight part of g: (la - <w, la>) * w / scale (projection :1093-1098, chain rule
+// :1125-1128, scaling :1135-1136).  One histogram per thread.
+__global__ void k_project_weights(const double* __restrict__ la, const double* __restrict__ w,
+                                  double* __restrict__ g, int P, int K, double scale) {
+  GRID_STRIDE(p, (size_t)P) {
+    double d = 0;
+    for (int k = 0; k < K; ++k) d += w[p * K + k] * la[p * K + k];
+    for (int k = 0; k < K; ++k) g[p * K + k] = ((la[p * K + k] - d) * w[p * K + k]) / scale;
+  }
+}
+
+// Atom part of g: (G - <atom, G>) * atom (:1103-1108, :1125-1128), block per atom.
+__global__ void k_project_atoms(const double* __restrict__ dic, const double* __restrict__ atoms,
+                                double* __restrict__ g, size_t N) {
+  __shared__ double sh[32];
+  const size_t k = blockIdx.x;
+  double d = 0;
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x) d += atoms[k * N + j] * dic[k * N + j];
+  d = block_sum(d, sh);
+  if (threadIdx.x == 0) sh[0] = d;
+  __syncthreads();
+  d = sh[0];
+  for (size_t j = threadIdx.x; j < N; j += blockDim.x)
+    g[k * N + j] = (dic[k * N + j] - d) * atoms[k * N + j];
+}
+
+__global__ void k_sum_losses(const double* __restrict__ loss, double* __restrict__ f, int P) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double s = 0;
+    for (int p = 0; p < P; ++p) s += loss[p];
+    *f = s;
+  }
+}
+
+// ---------------- workspace -----------------------------------------------------------
+inline void alloc_into(Arena& a, void** p, size_t bytes) { *p = a.take<char>(bytes); }
+inline void alloc_into(ArenaPlan& a, void** p, size_t bytes) {
+  a.take<char>(bytes);
+  *p = nullptr;
+}
+
+// Device workspace of one gradient_both call.  Pairs that feed one operator
+// launch (buf2 = [tmp | u], cbuf2, the sign arrays sd/sw) are single
+// allocations so that their halves are adjacent.
+template <typename T>
+struct EvalBufs {
+  T *atoms, *lam, *tape_b, *tape_cb, *tape_phi, *a, *bary, *n, *gw, *buf2, *cbuf2, *v, *r, *ctmp;
+  T *wa = nullptr, *wb = nullptr, *wc = nullptr, *wgrad = nullptr;
+  double *atoms64, *lam64, *gdic, *dot, *loss;
+  uint8_t *sd = nullptr, *sw = nullptr, *stmp = nullptr;
+
+  template <class A>
+  void layout(A& al, size_t P, size_t K, size_t L, size_t N, bool log_domain, bool wloss) {
+    const size_t KN = K * N, PKN = P * KN, PN = P * N;
+    auto t = [&](T*& p, size_t n) { alloc_into(al, reinterpret_cast<void**>(&p), n * sizeof(T)); };
+    auto d = [&](double*& p, size_t n) { alloc_into(al, reinterpret_cast<void**>(&p), n * 8); };
+    t(atoms, KN);
+    t(lam, P * K);
+    t(tape_b, (L + 1) * PKN);
+    t(tape_cb, L * PKN);
+    t(tape_phi, L * PKN);
+    t(a, PKN);
+    t(bary, PN);
+    t(n, PN);
+    t(gw, PN);
+    t(buf2, 2 * PKN);
+    t(cbuf2, 2 * PKN);
+    t(v, PKN);
+    t(r, PKN);
+    t(ctmp, 2 * PKN);
+    d(atoms64, KN);
+    d(lam64, P * K);
+    d(gdic, PKN);
+    d(dot, P * K);
+    d(loss, P);
+    if (wloss) {
+      t(wa, PN);
+      t(wb, PN);
+      t(wc, PN);
+      t(wgrad, PN);
+    }
+    if (log_domain) {
+      alloc_into(al, reinterpret_cast<void**>(&sd), 2 * PKN);
+      alloc_into(al, reinterpret_cast<void**>(&stmp), 2 * PKN);
+      sw = sd ? sd + PKN : nullptr;
+    }
+  }
+};
+
+template <typename T>
+size_t eval_bytes_t(size_t P, size_t K, size_t L, size_t N, bool log_domain, bool wloss) {
+  ArenaPlan plan;
+  EvalBufs<T> b;
+  b.layout(plan, P, K, L, N, log_domain, wloss);
+  return plan.off + 256;
+}
+
+int launch_cfg(wdl_ctx* ctx, size_t n) { return grid_for(n, 256, ctx->sm_count, 8); }
+
+// Nested Sinkhorn of the Wasserstein loss (cpp/loss.h:92-154) on all P
+// barycenters at once, kernel domain, 50 inner iterations.
+template <typename T>
+int wasserstein_loss(wdl_ctx* ctx, EvalBufs<T>& B, const double* obs, int P, cudaStream_t s) {
+  const size_t N = ctx->N, PN = (size_t)P * N;
+  const unsigned G = launch_cfg(ctx, PN);
+  int rc;
+  k_fill<T><<<G, 256, 0, s>>>(B.wb, T(1), PN);
+  WDL_LAUNCH_CHECK(ctx);
+  for (int it = 0; it < 50; ++it) {
+    if ((rc = conv_stack<T>(ctx, B.wb, B.wc, B.ctmp, P, s))) return rc;
+    k_ratio<T><<<G, 256, 0, s>>>(B.bary, nullptr, B.wc, B.wa, PN);
+    WDL_LAUNCH_CHECK(ctx);
+    if ((rc = conv_stack<T>(ctx, B.wa, B.wc, B.ctmp, P, s))) return rc;
+    k_ratio<T><<<G, 256, 0, s>>>(nullptr, obs, B.wc, B.wb, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if ((rc = conv_stack<T>(ctx, B.wb, B.wc, B.ctmp, P, s))) return rc;
+  k_wloss<T><<<P, 256, 0, s>>>(B.bary, obs, B.wa, B.wb, B.wc, B.wgrad, B.loss, ctx->gamma, N);
+  WDL_LAUNCH_CHECK(ctx);
+  return WDL_OK;
+}
+
+template <typename T>
+int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                    const double* weights, const double* observed, const double* b_init,
+                    double* result_la, double* result_dic, double* bary_out, double* loss_out,
+                    double* b_last, cudaStream_t s, bool normalise) {
+  const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
+  const bool wloss = loss_type == WDL_LOSS_WASSERSTEIN;
+  const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
+  int rc;
+  if ((rc = ensure_arena(ctx, eval_bytes_t<T>(P, K, L, N, log_domain, wloss)))) return rc;
+  ctx->arena.reset();
+  EvalBufs<T> B;
+  B.layout(ctx->arena, P, K, L, N, log_domain, wloss);
+  const unsigned G_PKN = launch_cfg(ctx, PKN), G_PN = launch_cfg(ctx, PN),
+                 G_2PKN = launch_cfg(ctx, 2 * PKN);
+
+  // Inputs: normalised FP64 copies (normalize_values, :562) and their T casts.
+  if (normalise) {
+    k_normalise_rows<<<K, 256, 0, s>>>(atoms, B.atoms64, N, 0.0);
+    WDL_LAUNCH_CHECK(ctx);
+    k_normalise_rows<<<P, 32, 0, s>>>(weights, B.lam64, K, 0.0);
+    WDL_LAUNCH_CHECK(ctx);
+  } else {
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(B.atoms64, atoms, KN * 8, cudaMemcpyDeviceToDevice, s));
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(B.lam64, weights, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  if (log_domain) k_log_of<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.atoms64, B.atoms, KN);
+  else k_cast<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.atoms64, B.atoms, KN);
+  WDL_LAUNCH_CHECK(ctx);
+  k_cast<T><<<1, 256, 0, s>>>(B.lam64, B.lam, (size_t)P * K);
+  WDL_LAUNCH_CHECK(ctx);
+  if (b_init) {
+    if (log_domain) k_log_of<T><<<G_PKN, 256, 0, s>>>(b_init, B.tape_b, PKN);
+    else k_cast<T><<<G_PKN, 256, 0, s>>>(b_init, B.tape_b, PKN);
+  } else {
+    k_fill<T><<<G_PKN, 256, 0, s>>>(B.tape_b, log_domain ? T(0) : T(1), PKN);
+  }
+  WDL_LAUNCH_CHECK(ctx);
+
+  // Forward Bregman projections, storing b, conv_b and phi (:565-593 / :700-720).
+  for (int it = 1; it <= L; ++it) {
+    const T* b_prev = B.tape_b + (size_t)(it - 1) * PKN;
+    T* cb = B.tape_cb + (size_t)(it - 1) * PKN;
+    T* phi = B.tape_phi + (size_t)(it - 1) * PKN;
+    T* b_next = B.tape_b + (size_t)it * PKN;
+    if (!log_domain) {
+      if ((rc = conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, s))) return rc;
+      k_div_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+      if ((rc = conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, s))) return rc;
+      k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam, b_next, B.bary, K, N, PN);
+    } else {
+      if ((rc = log_conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, nullptr, nullptr,
+                                  nullptr, s)))
+        return rc;
+      k_log_sub_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+      if ((rc = log_conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, nullptr, nullptr,
+                                  nullptr, s)))
+        return rc;
+      k_log_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam, b_next, B.bary, K, N, PN);
+    }
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if (log_domain) {
+    k_exp_inplace<T><<<G_PN, 256, 0, s>>>(B.bary, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+
+  // Loss and its gradient (:597).
+  if (wloss && (rc = wasserstein_loss<T>(ctx, B, observed, P, s))) return rc;
+  k_loss<T><<<P, 256, 0, s>>>(B.bary, observed, B.wgrad, B.n, B.gw, B.loss, loss_type, N);
+  WDL_LAUNCH_CHECK(ctx);
+
+  // Reverse pass, both recursions per round (:602-673 / :730-812).
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.v, 0, PKN * sizeof(T), s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.r, 0, PKN * sizeof(T), s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, PKN * sizeof(double), s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.dot, 0, (size_t)P * K * sizeof(double), s));
+  T* tmp = B.buf2;
+  T* u = B.buf2 + PKN;
+  for (int sstep = L; sstep >= 1; --sstep) {
+    const T* b_s = B.tape_b + (size_t)sstep * PKN;
+    const T* phi_s = B.tape_phi + (size_t)(sstep - 1) * PKN;
+    const T* cb_p = B.tape_cb + (size_t)(sstep - 1) * PKN;
+    const bool more = sstep > 1;
+    const size_t nimg = (size_t)(more ? 2 : 1) * P * K;
+    if (!log_domain) {
+      k_bwd_pre<T><<<P * K, 256, 0, s>>>(B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dot, K, N);
+      WDL_LAUNCH_CHECK(ctx);
+      if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
+      k_bwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, PKN, more);
+      WDL_LAUNCH_CHECK(ctx);
+      if (!more) break;
+      if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
+      const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
+      const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
+      k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+    } else {
+      k_lbwd_pre<T><<<P * K, 256, 0, s>>>(B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.sd,
+                                          B.sw, B.dot, K, N);
+      WDL_LAUNCH_CHECK(ctx);
+      // sd and sw are adjacent, so the pair is one 2*P*K-image signed operand.
+      if ((rc = log_conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, B.sd, B.sd, B.stmp, s)))
+        return rc;
+      k_lbwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.sd, B.gdic, B.buf2, KN, PKN,
+                                          more);
+      WDL_LAUNCH_CHECK(ctx);
+      if (!more) break;
+      if ((rc = log_conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, B.sd, B.sd, B.stmp, s)))
+        return rc;
+      const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
+      const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
+      k_lbwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.sd, B.sw, B.v, B.r, B.n, B.gw,
+                                          K, N, PN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+    }
+  }
+
+  // Outputs.
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
+  k_sum_over_p<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
+  WDL_LAUNCH_CHECK(ctx);
+  if (bary_out) {
+    k_cast_back<T><<<G_PN, 256, 0, s>>>(B.bary, bary_out, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if (loss_out) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(loss_out, B.loss, (size_t)P * 8, cudaMemcpyDeviceToDevice, s));
+  if (b_last) {
+    const T* bl = B.tape_b + (size_t)L * PKN;
+    if (log_domain) {
+      return set_error(ctx, WDL_ERR_UNSUPPORTED, "warm restart store is kernel-domain only (as the reference)");
+    }
+    k_cast_back<T><<<G_PKN, 256, 0, s>>>(bl, b_last, PKN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  return WDL_OK;
+}
+
+// Forward-only barycenter for P weight vectors (cpp/inverseWasserstein.h:115-201).
+template <typename T>
+int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
+                 double* bary_out, cudaStream_t s) {
+  const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
+  const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
+  int rc;
+  if ((rc = ensure_arena(ctx, barycenter_bytes(ctx, P, K)))) return rc;
+  ctx->arena.reset();
+  Arena& A = ctx->arena;
+  double* atoms64 = A.take<double>(KN);
+  double* lam64 = A.take<double>((size_t)P * K);
+  T* at = A.take<T>(KN);
+  T* lam = A.take<T>((size_t)P * K);
+  T* b = A.take<T>(PKN);
+  T* conv = A.take<T>(PKN);
+  T* a = A.take<T>(PKN);
+  T* tmp = A.take<T>(PKN);
+  T* bary = A.take<T>(PN);
+  k_normalise_rows<<<K, 256, 0, s>>>(atoms, atoms64, N, 0.0);
+  WDL_LAUNCH_CHECK(ctx);
+  k_normalise_rows<<<P, 32, 0, s>>>(weights, lam64, K, 0.0);
+  WDL_LAUNCH_CHECK(ctx);
+  if (log_domain) k_log_of<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(atoms64, at, KN);
+  else k_cast<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(atoms64, at, KN);
+  WDL_LAUNCH_CHECK(ctx);
+  k_cast<T><<<1, 256, 0, s>>>(lam64, lam, (size_t)P * K);
+  WDL_LAUNCH_CHECK(ctx);
+  k_fill<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(b, log_domain ? T(0) : T(1), PKN);
+  WDL_LAUNCH_CHECK(ctx);
+  for (int it = 0; it < L; ++it) {
+    if (!log_domain) {
+      if ((rc = conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, s))) return rc;
+      k_div_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+      if ((rc = conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, s))) return rc;
+      k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam, b, bary, K, N, PN);
+    } else {
+      if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
+        return rc;
+      k_log_sub_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN);
+      WDL_LAUNCH_CHECK(ctx);
+      if ((rc = log_conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
+        return rc;
+      k_log_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam, b, bary, K, N, PN);
+    }
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if (log_domain) {
+    k_exp_inplace<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(bary, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  k_cast_back<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(bary, bary_out, PN);
+  WDL_LAUNCH_CHECK(ctx);
+  return WDL_OK;
+}
+
+bool use_fp64(const wdl_ctx* ctx) { return ctx->precision == WDL_FP64; }
+
+}  // namespace
+
+size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L) {
+  const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
+  return use_fp64(ctx) ? eval_bytes_t<double>(P, K, L, ctx->N, log_domain, true)
+                       : eval_bytes_t<float>(P, K, L, ctx->N, log_domain, true);
+}
+
+size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K) {
+  const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
+  const size_t t = use_fp64(ctx) ? 8 : 4;
+  return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 16 * 256;
+}
+
+int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                      const double* weights, const double* observed, const double* b_init,
+                      double* result_la, double* result_dic, double* bary, double* loss,
+                      double* b_last, cudaStream_t s, bool normalise) {
+  if (use_fp64(ctx))
+    return gradient_both_t<double>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
+                                   result_la, result_dic, bary, loss, b_last, s, normalise);
+  return gradient_both_t<float>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
+                                result_la, result_dic, bary, loss, b_last, s, normalise);
+}
+
+int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
+                   double* bary, cudaStream_t s) {
+  if (use_fp64(ctx)) return barycenter_t<double>(ctx, P, K, L, atoms, weights, bary, s);
+  return barycenter_t<float>(ctx, P, K, L, atoms, weights, bary, s);
+}
+
+// evaluate_both (cpp/inverseWasserstein.h:986-1145) on device.  The gradient_both
+// call allocates the arena first; the FP64 staging of this function lives in a
+// second, small allocation owned by the context's arena tail.
+int evaluate_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                      const double* x, double* g, int n, const double* observed, double* f,
+                      const double* b_storage, double* b_last, double* bary, cudaStream_t s) {
+  const size_t N = ctx->N, KN = (size_t)K * N, PK = (size_t)P * K;
+  if ((size_t)n != PK + KN) return set_error(ctx, WDL_ERR_INVALID_ARG, "n != P*K + K*N");
+  // Staging: v2 weights [PK], v2 atoms [KN], la [PK], dic [KN], loss [P].
+  const size_t stage = 8 * (2 * PK + 2 * KN + P) + 5 * 256;
+  const size_t main = eval_bytes(ctx, P, K, L);
+  int rc;
+  if ((rc = ensure_arena(ctx, main + stage))) return rc;
+  char* tail = static_cast<char*>(ctx->arena.ptr) + main;
+  auto carve = [&](size_t nd) {
+    double* p = reinterpret_cast<double*>(tail);
+    tail += ((nd * 8 + 255) / 256) * 256;
+    return p;
+  };
+  double* w2 = carve(PK);
+  double* a2 = carve(KN);
+  double* la = carve(PK);
+  double* dic = carve(KN);
+  double* loss = carve(P);
+  // Back to the original domain and normalise (:997-1031).
+  k_normalise_rows<<<P, 32, 0, s>>>(x, w2, K, scale_dic);
+  WDL_LAUNCH_CHECK(ctx);
+  k_normalise_rows<<<K, 256, 0, s>>>(x + PK, a2, N, 1.0);
+  WDL_LAUNCH_CHECK(ctx);
+  if ((rc = gradient_both_dev(ctx, P, K, L, loss_type, a2, w2, observed, b_storage, la, dic, bary,
+                              loss, b_last, s, true)))
+    return rc;
+  k_project_weights<<<grid_for(P, 128, ctx->sm_count), 128, 0, s>>>(la, w2, g, P, K, scale_dic);
+  WDL_LAUNCH_CHECK(ctx);
+  k_project_atoms<<<K, 256, 0, s>>>(dic, a2, g + PK, N);
+  WDL_LAUNCH_CHECK(ctx);
+  k_sum_losses<<<1, 32, 0, s>>>(loss, f, P);
+  WDL_LAUNCH_CHECK(ctx);
+  return WDL_OK;
+}
+
+}  // namespace wdl

@@ -1,0 +1,182 @@
+// Internal declarations of libwdl_b200: the context, its device workspace and
+// the launch helpers shared by the kernel files.  Not part of the ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/wdl.h"
+
+namespace wdl {
+
+// log(1e-250): the value safe_log(x) = log(max(EPSILON, x)) takes at x = 0
+// (cpp/loss.h:3-5, EPSILON at cpp/kernels.h:30).  Every positive FP32 number
+// exceeds 1e-250, so in FP32 safe_log(x) is log(x) for x > 0 and this constant
+// otherwise; in FP64 the floor is applied literally.
+constexpr double kLogEpsilon = -575.6462732485114;
+constexpr double kEpsilon = 1e-250;
+
+struct Status {
+  int code = WDL_OK;
+  std::string msg;
+};
+
+// Grow-only device arena: one cudaMalloc per high-water mark, reused by every
+// call of the same or smaller size.
+struct Arena {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  size_t off = 0;
+  void reset() { off = 0; }
+  template <typename T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(static_cast<char*>(ptr) + off);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+// Size of an arena plan: the same sequence of take<T>(n) calls without memory.
+struct ArenaPlan {
+  size_t off = 0;
+  template <typename T>
+  void take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    off += n * sizeof(T);
+  }
+};
+
+struct TcResources;  // tensor-core factor matrices (conv_tc.cu)
+
+}  // namespace wdl
+
+struct wdl_ctx {
+  int device = 0;
+  int W = 0, H = 0, D = 1;
+  int ndim = 2;
+  size_t N = 0;
+  double gamma = 0;
+  int precision = WDL_FP32;
+  int domain = WDL_DOMAIN_KERNEL;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+
+  // Dense Gibbs factor of each axis, G[i][j] = max(EPSILON, exp(-(i-j)^2/gamma)),
+  // stored row-major n x n in FP64 and FP32 (cpp/kernels.h:637-640).
+  int axis_len[3] = {0, 0, 0};
+  double* G64[3] = {nullptr, nullptr, nullptr};
+  float* G32[3] = {nullptr, nullptr, nullptr};
+
+  wdl::Arena arena;  // compute workspace (tape, scratch)
+  wdl::Arena io;     // staging of the host-pointer calls
+  wdl::TcResources* tc = nullptr;
+
+  std::string last_error;
+  long long launches = 0;
+
+  bool profiling = false;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  double conv_ms = 0;
+  long long conv_launches = 0;
+  double conv_images = 0;
+};
+
+namespace wdl {
+
+int set_error(wdl_ctx* ctx, int code, const std::string& msg);
+int cuda_error(wdl_ctx* ctx, cudaError_t e, const char* where);
+int ensure_arena(wdl_ctx* ctx, size_t bytes);
+
+#define WDL_CUDA_TRY(ctx, expr)                                    \
+  do {                                                             \
+    cudaError_t _e = (expr);                                       \
+    if (_e != cudaSuccess) return ::wdl::cuda_error(ctx, _e, #expr); \
+  } while (0)
+
+#define WDL_LAUNCH_CHECK(ctx)                                                   \
+  do {                                                                          \
+    (ctx)->launches++;                                                          \
+    cudaError_t _e = cudaGetLastError();                                        \
+    if (_e != cudaSuccess) return ::wdl::cuda_error(ctx, _e, "kernel launch");  \
+  } while (0)
+
+inline unsigned grid_for(size_t n, int block, int sm_count, int per_sm = 8) {
+  size_t g = (n + block - 1) / block;
+  size_t cap = (size_t)sm_count * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+// ---- separable operator (conv_simt.cu / conv_tc.cu) ----------------------------
+// out_v = G (*) in_v for nimg stacked images of the context's grid.  in and out
+// must not alias; tmp holds nimg*N elements.
+int conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                   cudaStream_t s);
+int conv_stack_f64(wdl_ctx* ctx, const double* in, double* out, double* tmp, size_t nimg,
+                   cudaStream_t s);
+int conv_stack_simt_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                        cudaStream_t s);
+// Log-sum-exp operator; signs (one byte per element, 1 = non-negative) are read
+// from in_sign and written to out_sign when non-null.
+int log_conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                       const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
+                       cudaStream_t s);
+int log_conv_stack_f64(wdl_ctx* ctx, const double* in, double* out, double* tmp, size_t nimg,
+                       const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
+                       cudaStream_t s);
+
+template <typename T>
+inline int conv_stack(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg, cudaStream_t s);
+template <>
+inline int conv_stack<float>(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                             cudaStream_t s) {
+  return conv_stack_f32(ctx, in, out, tmp, nimg, s);
+}
+template <>
+inline int conv_stack<double>(wdl_ctx* ctx, const double* in, double* out, double* tmp,
+                              size_t nimg, cudaStream_t s) {
+  return conv_stack_f64(ctx, in, out, tmp, nimg, s);
+}
+
+template <typename T>
+inline int log_conv_stack(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg,
+                          const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
+                          cudaStream_t s);
+template <>
+inline int log_conv_stack<float>(wdl_ctx* ctx, const float* in, float* out, float* tmp,
+                                 size_t nimg, const uint8_t* is, uint8_t* os, uint8_t* ts,
+                                 cudaStream_t s) {
+  return log_conv_stack_f32(ctx, in, out, tmp, nimg, is, os, ts, s);
+}
+template <>
+inline int log_conv_stack<double>(wdl_ctx* ctx, const double* in, double* out, double* tmp,
+                                  size_t nimg, const uint8_t* is, uint8_t* os, uint8_t* ts,
+                                  cudaStream_t s) {
+  return log_conv_stack_f64(ctx, in, out, tmp, nimg, is, os, ts, s);
+}
+
+// Tensor-core resources (conv_tc.cu).
+int tc_init(wdl_ctx* ctx);
+void tc_free(wdl_ctx* ctx);
+bool tc_supported(const wdl_ctx* ctx);
+
+// Hot path entry points (sinkhorn.cu); all pointers are device pointers.
+int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                      const double* weights, const double* observed, const double* b_init,
+                      double* result_la, double* result_dic, double* bary, double* loss,
+                      double* b_last, cudaStream_t s, bool normalise);
+int evaluate_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                      const double* x, double* g, int n, const double* observed, double* f,
+                      const double* b_storage, double* b_last, double* bary, cudaStream_t s);
+int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
+                   double* bary, cudaStream_t s);
+size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L);
+size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K);
+
+}  // namespace wdl
