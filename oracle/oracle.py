@@ -81,6 +81,11 @@ class OracleLib:
                                         C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp,
                                         _dp, _dp, _dp, C.c_int]
         L.orc_evaluate_both.restype = C.c_double
+        L.orc_gradient_both_scale.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                                              C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_weight_gradient_scale.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                                                C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                _dp, _dp, _dp, C.c_int]
 
     def convolve(self, W, H, D, gamma, u, nv):
         u = np.ascontiguousarray(u, dtype=np.float64)
@@ -124,6 +129,28 @@ class OracleLib:
         if want_b_last:
             return la, dic, bary, b_last
         return la, dic, bary
+
+    def gradient_both_scale(self, W, H, D, gamma, K, L, loss_type, atoms, lambdas, obs,
+                            log_domain=False):
+        """Mass of the terms summed into resultLa (its floating-point condition scale)."""
+        atoms = np.ascontiguousarray(atoms, dtype=np.float64)
+        lambdas = np.ascontiguousarray(lambdas, dtype=np.float64)
+        obs = np.ascontiguousarray(obs, dtype=np.float64)
+        out = np.zeros(K)
+        self.L.orc_gradient_both_scale(W, H, D, gamma, K, L, loss_type, int(log_domain), _p(atoms),
+                                       _p(lambdas), _p(obs), _p(out))
+        return out
+
+    def weight_gradient_scale(self, W, H, D, gamma, P, K, L, loss_type, scale_dic, x, obs,
+                              log_domain=False, nthreads=None):
+        """Per-entry error scale of evaluate_both's weight gradient (see wdl_oracle.h)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        obs = np.ascontiguousarray(obs, dtype=np.float64)
+        out = np.zeros(P * K)
+        self.L.orc_weight_gradient_scale(W, H, D, gamma, P, K, L, loss_type, int(log_domain),
+                                         scale_dic, _p(x), _p(obs), _p(out),
+                                         nthreads or os.cpu_count() or 1)
+        return out
 
     def gradient_both_log(self, W, H, gamma, K, L, loss_type, atoms, lambdas, obs):
         N = W * H
@@ -245,6 +272,28 @@ class RefLib:
         self.K.ref_gradient_both(kind, gamma, W, H, D, K, L, loss_type, _p(atoms), _p(lambdas),
                                  _p(obs), _p(la), _p(dic), _p(bary))
         return la, dic, bary
+
+    def gradient_both_scale(self, W, H, D, gamma, K, L, loss_type, atoms, lambdas, obs,
+                            log_domain=False):
+        """Mass of the terms summed into resultLa (its floating-point condition scale)."""
+        atoms = np.ascontiguousarray(atoms, dtype=np.float64)
+        lambdas = np.ascontiguousarray(lambdas, dtype=np.float64)
+        obs = np.ascontiguousarray(obs, dtype=np.float64)
+        out = np.zeros(K)
+        self.L.orc_gradient_both_scale(W, H, D, gamma, K, L, loss_type, int(log_domain), _p(atoms),
+                                       _p(lambdas), _p(obs), _p(out))
+        return out
+
+    def weight_gradient_scale(self, W, H, D, gamma, P, K, L, loss_type, scale_dic, x, obs,
+                              log_domain=False, nthreads=None):
+        """Per-entry error scale of evaluate_both's weight gradient (see wdl_oracle.h)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        obs = np.ascontiguousarray(obs, dtype=np.float64)
+        out = np.zeros(P * K)
+        self.L.orc_weight_gradient_scale(W, H, D, gamma, P, K, L, loss_type, int(log_domain),
+                                         scale_dic, _p(x), _p(obs), _p(out),
+                                         nthreads or os.cpu_count() or 1)
+        return out
 
     def gradient_both_log(self, W, H, gamma, K, L, loss_type, atoms, lambdas, obs):
         N = W * H

@@ -199,10 +199,10 @@ static void normalized_copy(const double* atoms, const double* lambdas, int K, s
   }
 }
 
-void orc_gradient_both(int W, int H, int D, double gamma, int K, int L, int loss_type,
-                       const double* atoms, const double* lambdas, const double* obs,
-                       const double* b_init, double* resultLa, double* resultDic,
-                       double* bary, double* b_last) {
+static void gradient_both_impl(int W, int H, int D, double gamma, int K, int L, int loss_type,
+                               const double* atoms, const double* lambdas, const double* obs,
+                               const double* b_init, double* resultLa, double* resultDic,
+                               double* bary, double* b_last, double* la_abs) {
   const size_t N = (size_t)W * H * D, KN = (size_t)K * N;
   double* p = xalloc(KN);
   double* lam = xalloc(K);
@@ -269,11 +269,14 @@ void orc_gradient_both(int W, int H, int D, double gamma, int K, int L, int loss
   double* u = xalloc(KN);
   double* convu = xalloc(KN);
   for (int k = 0; k < K; ++k) resultLa[k] = 0;
+  if (la_abs)
+    for (int k = 0; k < K; ++k) la_abs[k] = 0;
   for (int s = L; s >= 1; --s) {
     const double* ph = phi + (size_t)s * KN;
     for (int k = 0; k < K; ++k) {
       double dotp = 0;
       for (size_t j = 0; j < N; ++j) {
+        if (la_abs) la_abs[k] += fabs(log(ph[k * N + j]) * g[j]);
         dotp += log(ph[k * N + j]) * g[j];
         u[k * N + j] = (lam[k] * g[j] - r[k * N + j]) / ph[k * N + j];
       }
@@ -303,9 +306,10 @@ static inline double abs_exp(double lv, const unsigned char* s, size_t i) { /* :
   return get_sign(s, i) * exp(lv);
 }
 
-void orc_gradient_both_log(int W, int H, double gamma, int K, int L, int loss_type,
-                           const double* atoms, const double* lambdas, const double* obs,
-                           double* resultLa, double* resultDic, double* bary) {
+static void gradient_both_log_impl(int W, int H, double gamma, int K, int L, int loss_type,
+                                   const double* atoms, const double* lambdas, const double* obs,
+                                   double* resultLa, double* resultDic, double* bary,
+                                   double* la_abs) {
   const size_t N = (size_t)W * H, KN = (size_t)K * N;
   double* p = xalloc(KN);
   double* lam = xalloc(K);
@@ -371,12 +375,15 @@ void orc_gradient_both_log(int W, int H, double gamma, int K, int L, int loss_ty
   double* u = xalloc(KN);
   double* convu = xalloc(KN);
   for (int k = 0; k < K; ++k) resultLa[k] = 0;
+  if (la_abs)
+    for (int k = 0; k < K; ++k) la_abs[k] = 0;
   for (int s = L; s >= 1; --s) {
     const double* ph = phi + (size_t)s * KN;
     for (int k = 0; k < K; ++k) {
       double dotp = 0;
       for (size_t j = 0; j < N; ++j) {
         size_t i = k * N + j;
+        if (la_abs) la_abs[k] += fabs(ph[i] * g[j]);
         dotp += ph[i] * g[j];
         u[i] = abs_log(lam[k] * g[j] + r[i], sg, i) - ph[i];
       }
@@ -397,6 +404,38 @@ void orc_gradient_both_log(int W, int H, double gamma, int K, int L, int loss_ty
   free(sg);
   free(p); free(lam); free(b); free(conv_b); free(phi); free(a); free(g);
   free(n); free(v); free(tmp); free(c); free(sumv); free(r); free(u); free(convu);
+}
+
+void orc_gradient_both(int W, int H, int D, double gamma, int K, int L, int loss_type,
+                       const double* atoms, const double* lambdas, const double* obs,
+                       const double* b_init, double* resultLa, double* resultDic,
+                       double* bary, double* b_last) {
+  gradient_both_impl(W, H, D, gamma, K, L, loss_type, atoms, lambdas, obs, b_init, resultLa,
+                     resultDic, bary, b_last, NULL);
+}
+
+void orc_gradient_both_log(int W, int H, double gamma, int K, int L, int loss_type,
+                           const double* atoms, const double* lambdas, const double* obs,
+                           double* resultLa, double* resultDic, double* bary) {
+  gradient_both_log_impl(W, H, gamma, K, L, loss_type, atoms, lambdas, obs, resultLa, resultDic,
+                         bary, NULL);
+}
+
+void orc_gradient_both_scale(int W, int H, int D, double gamma, int K, int L, int loss_type,
+                             int log_domain, const double* atoms, const double* lambdas,
+                             const double* obs, double* la_abs) {
+  const size_t N = (size_t)W * H * D;
+  double* la = xalloc(K);
+  double* dic = xalloc((size_t)K * N);
+  double* bary = xalloc(N);
+  if (log_domain)
+    gradient_both_log_impl(W, H, gamma, K, L, loss_type, atoms, lambdas, obs, la, dic, bary, la_abs);
+  else
+    gradient_both_impl(W, H, D, gamma, K, L, loss_type, atoms, lambdas, obs, NULL, la, dic, bary,
+                       NULL, la_abs);
+  free(la);
+  free(dic);
+  free(bary);
 }
 
 void orc_barycenter(int W, int H, int D, double gamma, int K, int L, const double* atoms,
@@ -507,4 +546,38 @@ double orc_evaluate_both(int W, int H, int D, double gamma, int P, int K, int L,
   free(gdic);
   free(losses);
   return lossVal;
+}
+
+void orc_weight_gradient_scale(int W, int H, int D, double gamma, int P, int K, int L,
+                               int loss_type, int log_domain, double scale_dic, const double* x,
+                               const double* obs, double* gw_scale, int nthreads) {
+  const size_t N = (size_t)W * H * D, KN = (size_t)K * N, PK = (size_t)P * K;
+  double* w = xalloc(PK);
+  double* a = xalloc(KN);
+  for (size_t i = 0; i < PK; ++i) w[i] = exp(x[i] / scale_dic);
+  for (size_t i = 0; i < KN; ++i) a[i] = exp(x[PK + i]);
+  for (int p = 0; p < P; ++p) {
+    double s = 0;
+    for (int k = 0; k < K; ++k) s += w[p * K + k];
+    for (int k = 0; k < K; ++k) w[p * K + k] /= s;
+  }
+  for (int k = 0; k < K; ++k) {
+    double s = 0;
+    for (size_t j = 0; j < N; ++j) s += a[k * N + j];
+    for (size_t j = 0; j < N; ++j) a[k * N + j] /= s;
+  }
+#ifdef _OPENMP
+  if (nthreads < 1) nthreads = 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int p = 0; p < P; ++p) {
+    double la_abs[64];
+    orc_gradient_both_scale(W, H, D, gamma, K, L, loss_type, log_domain, a, w + (size_t)p * K,
+                            obs + (size_t)p * N, la_abs);
+    double m = 0;
+    for (int k = 0; k < K; ++k) m += w[p * K + k] * la_abs[k];
+    for (int k = 0; k < K; ++k) gw_scale[p * K + k] = (la_abs[k] + m) * w[p * K + k] / scale_dic;
+  }
+  free(w);
+  free(a);
 }

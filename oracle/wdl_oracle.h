@@ -49,6 +49,15 @@ void orc_gradient_both(int W, int H, int D, double gamma, int K, int L, int loss
                        const double* b_init, double* resultLa, double* resultDic,
                        double* bary, double* b_last);
 
+/* Condition scale of resultLa: la_abs[k] = sum over steps s and pixels j of
+ * |log(phi[s]_kj) g_j| (log domain: |phi g|), the mass of the terms whose sum is
+ * resultLa[k].  A floating-point evaluation of resultLa is accurate to a small
+ * multiple of unit roundoff times la_abs, not times |resultLa|, which can be far
+ * smaller after cancellation.  Test infrastructure only. */
+void orc_gradient_both_scale(int W, int H, int D, double gamma, int K, int L, int loss_type,
+                             int log_domain, const double* atoms, const double* lambdas,
+                             const double* obs, double* la_abs);
+
 /* compute_gradient_both_log_signArray (cpp/inverseWasserstein.h:678-814). */
 void orc_gradient_both_log(int W, int H, double gamma, int K, int L, int loss_type,
                            const double* atoms, const double* lambdas, const double* obs,
@@ -70,6 +79,14 @@ double orc_evaluate_both(int W, int H, int D, double gamma, int P, int K, int L,
                          int log_domain, double scale_dic, const double* x, double* g,
                          const double* obs, const double* b_storage, double* b_last,
                          double* bary_out, int nthreads);
+
+/* Condition scale of evaluate_both's weight gradient (test infrastructure):
+ * gw_scale[p*K+k] = (la_abs_pk + sum_j w_pj la_abs_pj) * w_pk / scale_dic, the
+ * error bound of g[p*K+k] = (la_pk - <w_p, la_p>) w_pk / scale_dic in units of
+ * the relative error of the la terms. */
+void orc_weight_gradient_scale(int W, int H, int D, double gamma, int P, int K, int L,
+                               int loss_type, int log_domain, double scale_dic, const double* x,
+                               const double* obs, double* gw_scale, int nthreads);
 
 #ifdef __cplusplus
 }

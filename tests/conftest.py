@@ -30,6 +30,15 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
+def rel_scaled(a, b, scale):
+    """max|a-b| / max(scale): error against the mass of the terms summed into b
+    (its floating-point condition scale), for outputs that are differences of
+    near-equal sums (the weight gradients)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(scale))), 1e-300))
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle.oracle import OracleLib

@@ -226,10 +226,7 @@ int wdl_create(wdl_ctx** out, int device, int W, int H, int D, double gamma, int
   if (e != cudaSuccess) rc = cuda_error(ctx, e, "stream/event creation");
   if (rc == WDL_OK) rc = build_factors(ctx);
   if (rc == WDL_OK && (precision == WDL_TF32 || precision == WDL_SPLIT_BF16)) {
-    if (!tc_supported(ctx))
-      rc = set_error(ctx, WDL_ERR_UNSUPPORTED,
-                     "tensor-core operator needs every grid side <= 256 and a 2-D grid");
-    else rc = tc_init(ctx);
+    rc = tc_init(ctx);
   }
   if (rc != WDL_OK) {
     g_create_error = ctx->last_error;
@@ -261,7 +258,7 @@ int wdl_destroy(wdl_ctx* ctx) {
 int wdl_synchronize(wdl_ctx* ctx) {
   if (!ctx) return WDL_ERR_INVALID_ARG;
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  return WDL_OK;
+  return tc_check_status(ctx);
 }
 
 size_t wdl_eval_bytes(const wdl_ctx* ctx, int P, int K, int L) {
@@ -314,7 +311,7 @@ int wdl_convolve(wdl_ctx* ctx, const double* u, double* out, int nvectors) {
   if ((rc = wdl_convolve_device(ctx, du, dout, nvectors, ctx->stream))) return rc;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  return WDL_OK;
+  return tc_check_status(ctx);
 }
 
 static int log_convolve_common(wdl_ctx* ctx, const double* u, unsigned char* signs, double* out,
@@ -422,7 +419,7 @@ int wdl_gradient_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
   if (loss) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(loss, d_loss, P * 8, cudaMemcpyDeviceToHost, s));
   if (b_last) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(b_last, d_blast, PKN * 8, cudaMemcpyDeviceToHost, s));
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-  return WDL_OK;
+  return tc_check_status(ctx);
 }
 
 int wdl_evaluate_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
@@ -472,6 +469,7 @@ int wdl_evaluate_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double s
   if (bary) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(bary, d_bary, PN * 8, cudaMemcpyDeviceToHost, s));
   if (b_last) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(b_last, d_bl, PKN * 8, cudaMemcpyDeviceToHost, s));
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  if ((rc = tc_check_status(ctx))) return rc;
   if (!std::isfinite(*f)) return set_error(ctx, WDL_ERR_NONFINITE, "objective is not finite");
   return WDL_OK;
 }
@@ -496,7 +494,7 @@ int wdl_barycenter(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const
   if ((rc = barycenter_dev(ctx, P, K, L, d_atoms, d_w, d_bary, s))) return rc;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(bary, d_bary, PN * 8, cudaMemcpyDeviceToHost, s));
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-  return WDL_OK;
+  return tc_check_status(ctx);
 }
 
 }  // extern "C"

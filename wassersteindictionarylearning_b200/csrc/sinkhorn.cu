@@ -16,6 +16,7 @@
 #include <cmath>
 
 #include "wdl_internal.cuh"
+#include "wdl_math.cuh"
 
 namespace wdl {
 namespace {
@@ -44,6 +45,34 @@ template <>
 __device__ __forceinline__ float safe_log<float>(float x) {
   return x > 0.f ? logf(x) : float(kLogEpsilon);
 }
+
+// Logarithms that are summed in FP64 (grid reductions, the geometric mean over
+// atoms): FP64 mode uses log directly; FP32 mode uses the split form of
+// log_f32_precise so the FP64 sum is not limited by logf's absolute error.
+template <typename T>
+__device__ __forceinline__ double acc_log(T x);
+template <>
+__device__ __forceinline__ double acc_log<double>(double x) { return log(x); }
+template <>
+__device__ __forceinline__ double acc_log<float>(float x) {
+  return x > 0.f ? log_f32_precise(x) : (double)logf(x);
+}
+template <typename T>
+__device__ __forceinline__ double acc_safe_log(T x);
+template <>
+__device__ __forceinline__ double acc_safe_log<double>(double x) {
+  return log(x > kEpsilon ? x : kEpsilon);
+}
+template <>
+__device__ __forceinline__ double acc_safe_log<float>(float x) {
+  return x > 0.f ? log_f32_precise(x) : kLogEpsilon;
+}
+template <typename T>
+__device__ __forceinline__ T exp_from(double s);
+template <>
+__device__ __forceinline__ double exp_from<double>(double s) { return exp(s); }
+template <>
+__device__ __forceinline__ float exp_from<float>(double s) { return exp_to_f32(s); }
 
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -110,14 +139,14 @@ __global__ void k_div_atoms(const T* __restrict__ atoms, const T* __restrict__ c
 
 // Weighted geometric mean over the K atoms and the next scalings b = bary / phi.
 template <typename T>
-__global__ void k_bary_b(const T* __restrict__ phi, const T* __restrict__ lam, T* __restrict__ b,
-                         T* __restrict__ bary, int K, size_t N, size_t PN) {
+__global__ void k_bary_b(const T* __restrict__ phi, const double* __restrict__ lam,
+                         T* __restrict__ b, T* __restrict__ bary, int K, size_t N, size_t PN) {
   GRID_STRIDE(idx, PN) {
     const size_t p = idx / N, j = idx - p * N;
     const T* ph = phi + p * K * N + j;
-    T s = T(0);
-    for (int k = 0; k < K; ++k) s += safe_log<T>(ph[k * N]) * lam[p * K + k];
-    const T by = d_exp<T>(s);
+    double s = 0;
+    for (int k = 0; k < K; ++k) s += acc_safe_log<T>(ph[k * N]) * lam[p * K + k];
+    const T by = exp_from<T>(s);
     bary[idx] = by;
     if (b)
       for (int k = 0; k < K; ++k) b[p * K * N + k * N + j] = by / ph[k * N];
@@ -232,7 +261,7 @@ __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
     tmp[i] = (l * n[pb + j] - v[i]) * b_s[i];
     const T ph = phi_s[i];
     const T g = gw[pb + j];
-    acc += (double)d_log<T>(ph) * (double)g;
+    acc += acc_log<T>(ph) * (double)g;
     u[i] = (l * g - r[i]) / ph;
   }
   acc = block_sum(acc, sh);
@@ -528,7 +557,7 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       k_div_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN);
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, s))) return rc;
-      k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam, b_next, B.bary, K, N, PN);
+      k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam64, b_next, B.bary, K, N, PN);
     } else {
       if ((rc = log_conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, nullptr, nullptr,
                                   nullptr, s)))
@@ -654,7 +683,7 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
       k_div_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN);
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, s))) return rc;
-      k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam, b, bary, K, N, PN);
+      k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam64, b, bary, K, N, PN);
     } else {
       if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
         return rc;

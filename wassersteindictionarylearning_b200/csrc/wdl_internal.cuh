@@ -164,6 +164,9 @@ inline int log_conv_stack<double>(wdl_ctx* ctx, const double* in, double* out, d
 // Tensor-core resources (conv_tc.cu).
 int tc_init(wdl_ctx* ctx);
 void tc_free(wdl_ctx* ctx);
+// Reads and clears the status word the tensor-core kernels set when a bounded
+// wait gives up (WDL_ERR_TIMEOUT); WDL_OK otherwise.
+int tc_check_status(wdl_ctx* ctx);
 bool tc_supported(const wdl_ctx* ctx);
 
 // Hot path entry points (sinkhorn.cu); all pointers are device pointers.
