@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--precision", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    # Reduced sizes for profiler captures (the bench line itself uses the workload's).
+    ap.add_argument("--P", type=int, default=None)
+    ap.add_argument("--L", type=int, default=None)
     return ap.parse_args()
 
 
@@ -202,7 +205,11 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     precision = args.precision or default_precision()
-    wl = WORKLOAD
+    wl = dict(WORKLOAD)
+    if args.P:
+        wl["P"] = args.P
+    if args.L:
+        wl["L"] = args.L
     P, W, H, K, L = wl["P"], wl["W"], wl["H"], wl["K"], wl["L"]
     N = W * H
     cfg, obs, atoms, wts = make_problem(None, seed=1000 * rank, P=P, W=W, H=H, K=K, L=L,
@@ -219,7 +226,11 @@ def run_ours(args):
     obs_d = torch.from_numpy(obs.reshape(-1)).to(dev)
     g_d = torch.empty(n, dtype=torch.float64, device=dev)
     f_d = torch.empty(1, dtype=torch.float64, device=dev)
-    stream = torch.cuda.current_stream()
+    # An explicit stream: the library runs on it and the CUDA events below are
+    # recorded on it (handle 0, the legacy default stream, would mean "the
+    # context's own stream" to the C ABI).
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     sptr = C.c_void_p(stream.cuda_stream)
     fg = torch.empty(K * N + 1, dtype=torch.float64, device=dev)
 

@@ -268,3 +268,65 @@ def test_split_bf16_path_vs_oracle(oracle, case):
     assert abs(fv - f_ref) <= 1e-4 * abs(f_ref)
     check_gradient(oracle, g, g_ref, W, H, 1, cfg["gamma"], P, K, L, cfg["loss"], cfg["scale_dic"],
                    x, obs, 1e-3, 1e-3)
+
+
+@pytest.mark.parametrize("precision", ["split_bf16", "tf32"])
+def test_fused_gradient_both_vs_oracle(oracle, precision):
+    """Raw resultLa / resultDic / barycenters / losses of the persistent fused
+    kernel against the FP64 oracle, histogram by histogram."""
+    cfg, obs, x = _problem(P=5, W=48, H=40, K=3, L=15, gamma=1.5, loss=2)
+    W, H, P, K, L = cfg["W"], cfg["H"], cfg["P"], cfg["K"], cfg["L"]
+    from wassersteindictionarylearning_b200.synthetic import init_atoms, init_weights
+    atoms = init_atoms(K, W * H, seed=3)
+    w = init_weights(P, K, seed=4)
+    reg = _regression(W, H, 1, cfg["gamma"], P, K, L, 2, 1.0, obs, precision)
+    la, dic, bary, loss = reg.compute_gradient_both(atoms, w)
+    tol_b, tol_g = (1e-4, 1e-3) if precision == "split_bf16" else (3e-3, 2e-2)
+    dic_ref = np.zeros(K * W * H)
+    for p in range(P):
+        la_r, dic_r, bary_r = oracle.gradient_both(W, H, 1, cfg["gamma"], K, L, 2, atoms, w[p], obs[p])
+        f_r, _ = oracle.loss(2, W, H, 1, cfg["gamma"], bary_r, obs[p])
+        scale = oracle.gradient_both_scale(W, H, 1, cfg["gamma"], K, L, 2, atoms, w[p], obs[p])
+        assert rel(bary[p * W * H:(p + 1) * W * H], bary_r) < tol_b
+        assert abs(loss[p] - f_r) <= tol_b * abs(f_r)
+        assert rel_scaled(la[p * K:(p + 1) * K], la_r, scale) < tol_g
+        dic_ref += dic_r
+    assert rel(dic, dic_ref) < tol_g
+
+
+def test_fused_barycenter_and_warm_restart(oracle):
+    from wassersteindictionarylearning_b200 import Problem, WassersteinBarycenter
+    (_, f), = golden("bary_16x16x1_K3_L20_ker")
+    k = kern(float(f["gamma"]), 16, 16, 1, "split_bf16")
+    prob = Problem(f["atoms"], np.zeros(256), k, f["lambdas"], 1)
+    b = WassersteinBarycenter(prob, int(f["L"])).compute_barycenter()
+    assert rel(b, f["bary"]) < 1e-4
+    # several weight vectors at once (the serving batch form)
+    from wassersteindictionarylearning_b200.synthetic import init_weights
+    ws = init_weights(7, 3, seed=9)
+    bs = WassersteinBarycenter(prob, int(f["L"])).compute_barycenter(ws)
+    for i in range(7):
+        ref = oracle.barycenter(16, 16, 1, float(f["gamma"]), 3, int(f["L"]), f["atoms"], ws[i])
+        assert rel(bs[i], ref) < 1e-4
+    (_, f), = golden("warm_*")
+    W, H, P, K, L = (int(f[k]) for k in ("W", "H", "P", "K", "L"))
+    reg = _regression(W, H, 1, float(f["gamma"]), P, K, L, int(f["loss"]), float(f["scale_dic"]),
+                      f["obs"], "split_bf16")
+    reg.warmRestart = True
+    reg.b_storage = f["b_storage"].copy()
+    fv, g = reg.evaluate_both(f["x"])
+    assert abs(fv - float(f["f"])) <= 1e-4 * abs(float(f["f"]))
+    assert rel(reg.b_temp, f["b_last"]) < 1e-4
+    assert rel(g[P * K:], f["g"][P * K:]) < 1e-3
+
+
+def test_fused_wasserstein_loss_falls_back_to_operator_path(oracle):
+    """Loss type 3 (nested Sinkhorn) runs through the unfused tensor-core
+    operator path; results still match the oracle."""
+    cfg, obs, x = _problem(P=2, W=16, H=16, K=2, L=5, gamma=2.0, loss=3)
+    W, H, P, K, L = cfg["W"], cfg["H"], cfg["P"], cfg["K"], cfg["L"]
+    f_ref, g_ref = oracle.evaluate_both(W, H, 1, 2.0, P, K, L, 3, cfg["scale_dic"], x, obs)
+    reg = _regression(W, H, 1, 2.0, P, K, L, 3, cfg["scale_dic"], obs, "split_bf16")
+    fv, g = reg.evaluate_both(x)
+    assert abs(fv - f_ref) <= 1e-3 * abs(f_ref)
+    assert rel(g[P * K:], g_ref[P * K:]) < 1e-2

@@ -20,10 +20,7 @@
 // tiles use the canonical 128-byte-swizzled K-major layout: a tile of 128 rows
 // is split along K into 128-byte column blocks ("regions") of 128 x 128 B; in a
 // region, row r's 16-byte chunk c sits at chunk position c ^ (r % 8).
-#include <cuda_bf16.h>
-
-#include "tc_ptx.cuh"
-#include "wdl_internal.cuh"
+#include "tc_common.cuh"
 
 namespace wdl {
 
@@ -35,158 +32,119 @@ struct TcResources {
 
 namespace {
 
-constexpr int kRows = 128;               // tile rows (TMEM lanes / max grid side)
-constexpr int kRegionBytes = kRows * 128; // one 128-byte column block of a tile
-constexpr uint32_t kTmemCols = 256;      // D1: columns [0,128), D2: [128,256)
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on every mbarrier wait
-constexpr size_t kTileBytes = 64 * 1024;     // one operand (both planes)
+using namespace tc;
 
+// Image U (H x W fp32, row-major) -> operand tile rows i < Hp, K = k < Wp, zero
+// padded.  Work unit: one 16-byte SMEM chunk of one row (8 BF16 or 4 TF32
+// values); a thread issues the global loads of UNR chunks before converting any
+// of them so that many loads are in flight.
 template <bool SPLIT>
-struct Fmt {
-  static constexpr int esz = SPLIT ? 2 : 4;            // bytes per element
-  static constexpr int kstep = SPLIT ? 16 : 8;          // K per MMA instruction
-  static constexpr int plane_bytes = kRows * 128 * esz; // 32 KB (bf16) / 64 KB (tf32)
-  static constexpr uint32_t fmt = SPLIT ? 1u : 2u;
-};
-
-__device__ __forceinline__ uint32_t swz(int r, int k, int esz) {
-  const int per = 128 / esz;
-  const int region = k / per;
-  const int byte = (k - region * per) * esz;
-  const int chunk = (byte >> 4) ^ (r & 7);
-  return (uint32_t)(region * kRegionBytes + r * 128 + (chunk << 4) + (byte & 15));
-}
-
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-// Store one value at (r, k) of an operand tile (one or two planes).
-template <bool SPLIT>
-__device__ __forceinline__ void put1(uint8_t* tile, int r, int k, float v) {
-  if (SPLIT) {
-    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-    const uint32_t o = swz(r, k, 2);
-    *reinterpret_cast<__nv_bfloat16*>(tile + o) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(tile + Fmt<true>::plane_bytes + o) = lo;
-  } else {
-    *reinterpret_cast<uint32_t*>(tile + swz(r, k, 4)) = to_tf32(v);
-  }
-}
-
-// Store 16 consecutive K values (k0 % 16 == 0) of row r: whole 16-byte chunks.
-template <bool SPLIT>
-__device__ __forceinline__ void put16(uint8_t* tile, int r, int k0, const float (&v)[16]) {
-  if (SPLIT) {
-    uint32_t hi[8], lo[8];
+__device__ __forceinline__ void stage_image(uint8_t* tile, const float* __restrict__ src, int W,
+                                            int H, int Wp, int Hp, int t, bool vec) {
+  constexpr int CE = SPLIT ? 8 : 4;  // elements per chunk
+  constexpr int UNR = 8;
+  const int cpr = Wp / CE;           // chunks per row
+  const int total = Hp * cpr;
+  for (int base = t; base < total; base += 128 * UNR) {
+    float v[UNR][CE];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * t], v[2 * t + 1]);
-      const float2 hf = __bfloat1622float2(h);
-      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * t] - hf.x, v[2 * t + 1] - hf.y);
-      hi[t] = *reinterpret_cast<const uint32_t*>(&h);
-      lo[t] = *reinterpret_cast<const uint32_t*>(&l);
+    for (int u = 0; u < UNR; ++u) {
+      const int c = base + u * 128;
+      const int i = c / cpr, k0 = (c - i * cpr) * CE;
+      if (c < total && i < H) {
+        const float* row = src + (size_t)i * W;
+        if (vec && k0 + CE <= W) {
+#pragma unroll
+          for (int q = 0; q < CE; q += 4) {
+            const float4 f = __ldg(reinterpret_cast<const float4*>(row + k0 + q));
+            v[u][q] = f.x; v[u][q + 1] = f.y; v[u][q + 2] = f.z; v[u][q + 3] = f.w;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < CE; ++q) v[u][q] = (k0 + q < W) ? __ldg(row + k0 + q) : 0.f;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < CE; ++q) v[u][q] = 0.f;
+      }
     }
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const uint32_t o = swz(r, k0 + 8 * c, 2);
-      *reinterpret_cast<uint4*>(tile + o) = make_uint4(hi[4 * c], hi[4 * c + 1], hi[4 * c + 2], hi[4 * c + 3]);
-      *reinterpret_cast<uint4*>(tile + Fmt<true>::plane_bytes + o) =
-          make_uint4(lo[4 * c], lo[4 * c + 1], lo[4 * c + 2], lo[4 * c + 3]);
-    }
-  } else {
+    for (int u = 0; u < UNR; ++u) {
+      const int c = base + u * 128;
+      if (c >= total) break;
+      const int i = c / cpr, k0 = (c - i * cpr) * CE;
+      if (SPLIT) {
+        uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const uint32_t o = swz(r, k0 + 4 * c, 4);
-      *reinterpret_cast<uint4*>(tile + o) = make_uint4(to_tf32(v[4 * c]), to_tf32(v[4 * c + 1]),
-                                                       to_tf32(v[4 * c + 2]), to_tf32(v[4 * c + 3]));
+        for (int q = 0; q < 4; ++q) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v[u][2 * q], v[u][2 * q + 1]);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(v[u][2 * q] - hf.x, v[u][2 * q + 1] - hf.y);
+          hi[q] = *reinterpret_cast<const uint32_t*>(&h);
+          lo[q] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        const uint32_t o = swz(i, k0, 2);
+        *reinterpret_cast<uint4*>(tile + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(tile + Fmt<true>::plane_bytes + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      } else {
+        *reinterpret_cast<uint4*>(tile + swz(i, k0, 4)) =
+            make_uint4(to_tf32(v[u][0]), to_tf32(v[u][1]), to_tf32(v[u][2]), to_tf32(v[u][3]));
+      }
     }
   }
 }
 
-// D[128 x N] (+)= A[128 x K] * B[N x K]^T, A and B K-major tiles in SMEM.
+// Two warpgroups per CTA, each streaming its own images through the shared
+// tensor pipe (while one restages or stores, the other's GEMM runs).  Warp w
+// of warpgroup g owns TMEM lanes 32(w%4)..+31; slot g uses TMEM columns
+// [256g, 256g+256): D1 at +0, D2 at +128.  The factor tile G is shared.
 template <bool SPLIT>
-__device__ __forceinline__ void issue_gemm(uint32_t d_tmem, uint32_t a_tile, uint32_t b_tile,
-                                           int K, int N) {
-  using F = Fmt<SPLIT>;
-  const uint32_t id = ptx::idesc(F::fmt, 128, (uint32_t)N);
-  const int steps = K / F::kstep;
-  for (int ks = 0; ks < steps; ++ks) {
-    const uint32_t byte = (uint32_t)ks * 32u;
-    const uint32_t off = (byte >> 7) * kRegionBytes + (byte & 127u);
-    const uint64_t a = ptx::sw128_desc(a_tile + off);
-    const uint64_t b = ptx::sw128_desc(b_tile + off);
-    if (SPLIT) {
-      const uint64_t alo = ptx::sw128_desc(a_tile + F::plane_bytes + off);
-      const uint64_t blo = ptx::sw128_desc(b_tile + F::plane_bytes + off);
-      ptx::mma_bf16(d_tmem, a, b, id, ks > 0 ? 1u : 0u);
-      ptx::mma_bf16(d_tmem, a, blo, id, 1u);
-      ptx::mma_bf16(d_tmem, alo, b, id, 1u);
-    } else {
-      ptx::mma_tf32(d_tmem, a, b, id, ks > 0 ? 1u : 0u);
-    }
-  }
-}
-
-// One image per loop iteration; grid-stride over the batch.  128 threads: warp w
-// owns TMEM lanes 32w..32w+31 (x = 32w + lane).
-template <bool SPLIT>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(256, 1)
     tc_conv2d_kernel(const float* __restrict__ in, float* __restrict__ out, long long nimg, int W,
                      int H, int Wp, int Hp, const float* __restrict__ G, int Gn, int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* g_tile = base;
-  uint8_t* x_tile = base + kTileBytes;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * kTileBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + 2 * kTileBytes + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar_a = ptx::smem_addr(bar);
+  const int wg = warp >> 2, wt = tid & 127;
+  uint8_t* x_tile = base + (1 + wg) * kTileBytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 3 * kTileBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + 3 * kTileBytes + 16);
+  const uint32_t bar_a = ptx::smem_addr(&bars[wg]);
   const uint32_t g_a = ptx::smem_addr(g_tile), x_a = ptx::smem_addr(x_tile);
 
-  // Resident factor tile: G[r][k] = g(|r-k|) for r, k < Gn, zero elsewhere.
-  for (int e = tid; e < kRows * kRows; e += blockDim.x) {
-    const int r = e >> 7, k = e & 127;
-    const float v = (r < Gn && k < Gn) ? G[(size_t)r * Gn + k] : 0.f;
-    put1<SPLIT>(g_tile, r, k, v);
-  }
+  load_factor<SPLIT>(g_tile, G, Gn, tid, blockDim.x);
   if (tid == 0) {
-    ptx::mbar_init(bar_a, 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[1]), 1);
     ptx::fence_mbar_init();
   }
-  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tmem_slot), kTmemCols);
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tmem_slot), 2 * kTmemCols);
   ptx::fence_proxy_async_smem();
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem = *tmem_slot + (uint32_t)wg * kTmemCols;
   const uint32_t d1 = tmem, d2 = tmem + 128;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-  const int j = warp * 32 + lane;  // x coordinate owned by this thread
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+  const int j = (warp & 3) * 32 + lane;  // x coordinate owned by this thread
+  const bool vec = (W % 4) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
   uint32_t phase = 0;
   bool ok = true;
 
-  for (long long img = blockIdx.x; img < nimg && ok; img += gridDim.x) {
+  for (long long img = 2 * (long long)blockIdx.x + wg; img < nimg && ok; img += 2LL * gridDim.x) {
     const float* src = in + (size_t)img * W * H;
     float* dst = out + (size_t)img * W * H;
-    // U into the operand tile, zero-padded to Hp x Wp.
-    for (int e = tid; e < Hp * Wp; e += blockDim.x) {
-      const int i = e / Wp, k = e - i * Wp;
-      const float v = (i < H && k < W) ? src[(size_t)i * W + k] : 0.f;
-      put1<SPLIT>(x_tile, i, k, v);
-    }
+    stage_image<SPLIT>(x_tile, src, W, H, Wp, Hp, wt, vec);
     ptx::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+    wg_sync(wg);
+    if (wt == 0) {
       ptx::tc_fence_after();
       issue_gemm<SPLIT>(d1, g_a, x_a, Wp, Hp);
       ptx::mma_commit(bar_a);
     }
-    ok = __syncthreads_and(ptx::mbar_wait(bar_a, phase, kWaitNs)) != 0;
+    ok = wg_all(ptx::mbar_wait(bar_a, phase, kWaitNs), wg);
     phase ^= 1;
     ptx::tc_fence_after();
     // D1 -> SMEM as the K-major A operand of the second GEMM (row j, K = i).
@@ -198,13 +156,13 @@ __global__ void __launch_bounds__(128, 1)
     }
     ptx::tc_fence_before();
     ptx::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+    wg_sync(wg);
+    if (wt == 0) {
       ptx::tc_fence_after();
       issue_gemm<SPLIT>(d2, x_a, g_a, Hp, Hp);
       ptx::mma_commit(bar_a);
     }
-    ok = __syncthreads_and(ok && ptx::mbar_wait(bar_a, phase, kWaitNs)) != 0;
+    ok = wg_all(ok && ptx::mbar_wait(bar_a, phase, kWaitNs), wg);
     phase ^= 1;
     ptx::tc_fence_after();
     for (int c0 = 0; c0 < Hp; c0 += 16) {
@@ -218,25 +176,25 @@ __global__ void __launch_bounds__(128, 1)
       }
     }
     ptx::tc_fence_before();
-    __syncthreads();
+    wg_sync(wg);
   }
-  if (!ok && tid == 0) atomicExch(err, WDL_ERR_TIMEOUT);
+  if (!ok && wt == 0) atomicExch(err, WDL_ERR_TIMEOUT);
   __syncthreads();
   ptx::tc_fence_after();
-  if (warp == 0) ptx::tmem_dealloc(tmem, kTmemCols);
+  if (warp == 0) ptx::tmem_dealloc(*tmem_slot, 2 * kTmemCols);
 }
 
 }  // namespace
 
 bool tc_supported(const wdl_ctx* ctx) {
-  return ctx->ndim == 2 && ctx->W <= kRows && ctx->H <= kRows;
+  return ctx->ndim == 2 && ctx->W <= tc::kRows && ctx->H <= tc::kRows;
 }
 
 int tc_init(wdl_ctx* ctx) {
   if (!tc_supported(ctx))
     return set_error(ctx, WDL_ERR_UNSUPPORTED, "tensor-core operator needs a 2-D grid with sides <= 128");
   auto* r = new TcResources();
-  r->smem_bytes = 2 * kTileBytes + 1024 + 64;
+  r->smem_bytes = 3 * tc::kTileBytes + 1024 + 64;
   ctx->tc = r;
   WDL_CUDA_TRY(ctx, cudaMalloc(&r->d_err, sizeof(int)));
   WDL_CUDA_TRY(ctx, cudaMemset(r->d_err, 0, sizeof(int)));
@@ -261,12 +219,13 @@ static int conv_stack_tc(wdl_ctx* ctx, const float* in, float* out, size_t nimg,
   const int Wp = (W + 15) & ~15, Hp = (H + 15) & ~15;
   const int Gn = W >= H ? W : H;
   const float* G = ctx->G32[W >= H ? 0 : 1];
-  const unsigned grid = (unsigned)(nimg < (size_t)ctx->sm_count ? nimg : (size_t)ctx->sm_count);
+  const size_t pairs = (nimg + 1) / 2;
+  const unsigned grid = (unsigned)(pairs < (size_t)ctx->sm_count ? pairs : (size_t)ctx->sm_count);
   if (ctx->precision == WDL_SPLIT_BF16)
-    tc_conv2d_kernel<true><<<grid, 128, ctx->tc->smem_bytes, s>>>(in, out, (long long)nimg, W, H, Wp,
+    tc_conv2d_kernel<true><<<grid, 256, ctx->tc->smem_bytes, s>>>(in, out, (long long)nimg, W, H, Wp,
                                                                   Hp, G, Gn, ctx->tc->d_err);
   else
-    tc_conv2d_kernel<false><<<grid, 128, ctx->tc->smem_bytes, s>>>(in, out, (long long)nimg, W, H, Wp,
+    tc_conv2d_kernel<false><<<grid, 256, ctx->tc->smem_bytes, s>>>(in, out, (long long)nimg, W, H, Wp,
                                                                    Hp, G, Gn, ctx->tc->d_err);
   WDL_LAUNCH_CHECK(ctx);
   return WDL_OK;
@@ -295,6 +254,12 @@ int conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t
 // Reads and clears the device status word of the tensor-core kernels.
 int tc_check_status(wdl_ctx* ctx) {
   if (!ctx->tc) return WDL_OK;
+  if (ctx->fused_sync) {
+    int* sync = ctx->fused_sync;
+    ctx->fused_sync = nullptr;
+    int rc = sinkhorn_tc_status(ctx, sync);
+    if (rc) return rc;
+  }
   int h = 0;
   WDL_CUDA_TRY(ctx, cudaMemcpy(&h, ctx->tc->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h != 0) {

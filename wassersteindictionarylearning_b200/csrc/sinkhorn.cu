@@ -419,6 +419,28 @@ __global__ void k_sum_losses(const double* __restrict__ loss, double* __restrict
   }
 }
 
+__global__ void k_sum_over_p_f32(const float* __restrict__ gdic, double* __restrict__ out, int P,
+                                 size_t KN) {
+  GRID_STRIDE(i, KN) {
+    double s = 0;
+    for (int p = 0; p < P; ++p) s += (double)gdic[(size_t)p * KN + i];
+    out[i] = s;
+  }
+}
+
+// b[L] = bary[L] / phi[L] (the warm-restart store) from the fused path's tape,
+// where bary = exp(acc).
+__global__ void k_b_last(const float* __restrict__ acc, const float* __restrict__ phi,
+                         double* __restrict__ out, int K, size_t N, size_t PKN) {
+  GRID_STRIDE(i, PKN) {
+    const size_t p = i / ((size_t)K * N), j = i % N;
+    out[i] = (double)(expf(acc[p * N + j]) / phi[i]);
+  }
+}
+__global__ void k_exp_to_double(const float* __restrict__ acc, double* __restrict__ out, size_t n) {
+  GRID_STRIDE(i, n) out[i] = (double)expf(acc[i]);
+}
+
 // ---------------- workspace -----------------------------------------------------------
 inline void alloc_into(Arena& a, void** p, size_t bytes) { *p = a.take<char>(bytes); }
 inline void alloc_into(ArenaPlan& a, void** p, size_t bytes) {
@@ -704,17 +726,169 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
   return WDL_OK;
 }
 
+// Fused tensor-core path: one persistent kernel for forward, loss and reverse
+// pass (sinkhorn_tc.cu).  Inputs are normalised here in FP64 as above.
+struct FusedBufs {
+  double *atoms64, *lam64, *dot, *loss;
+  float *atoms, *lam, *b0, *cb, *phi, *acc, *nb, *gwb, *v, *r, *gdic;
+  int* sync;
+  template <class A>
+  void layout(A& al, size_t P, size_t K, size_t L, size_t N, bool b_init, bool fwd_only) {
+    const size_t KN = K * N, PKN = P * KN, PN = P * N, slots = fwd_only ? 2 : L;
+    auto f = [&](float*& p, size_t n) { alloc_into(al, reinterpret_cast<void**>(&p), n * 4); };
+    auto d = [&](double*& p, size_t n) { alloc_into(al, reinterpret_cast<void**>(&p), n * 8); };
+    d(atoms64, KN);
+    d(lam64, P * K);
+    d(dot, P * K);
+    d(loss, P);
+    f(atoms, KN);
+    f(lam, P * K);
+    b0 = nullptr;
+    if (b_init) f(b0, PKN);
+    f(cb, fwd_only ? 1 : slots * PKN);
+    f(phi, slots * PKN);
+    f(acc, slots * PN);
+    f(nb, fwd_only ? 1 : 2 * PN);
+    f(gwb, fwd_only ? 1 : 2 * PN);
+    f(v, fwd_only ? 1 : PKN);
+    f(r, fwd_only ? 1 : PKN);
+    f(gdic, fwd_only ? 1 : PKN);
+    alloc_into(al, reinterpret_cast<void**>(&sync), sk_sync_ints((int)P) * sizeof(int));
+  }
+};
+
+size_t fused_bytes(size_t P, size_t K, size_t L, size_t N, bool b_init, bool fwd_only) {
+  ArenaPlan plan;
+  FusedBufs b;
+  b.layout(plan, P, K, L, N, b_init, fwd_only);
+  return plan.off + 256;
+}
+
+bool use_fused(const wdl_ctx* ctx, int loss_type) {
+  return ctx->tc != nullptr && ctx->domain == WDL_DOMAIN_KERNEL && loss_type != WDL_LOSS_WASSERSTEIN;
+}
+
+int prepare_fused(wdl_ctx* ctx, FusedBufs& B, int P, int K, const double* atoms,
+                  const double* weights, const double* b_init, bool normalise, cudaStream_t s) {
+  const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN;
+  if (normalise) {
+    k_normalise_rows<<<K, 256, 0, s>>>(atoms, B.atoms64, N, 0.0);
+    WDL_LAUNCH_CHECK(ctx);
+    k_normalise_rows<<<P, 32, 0, s>>>(weights, B.lam64, K, 0.0);
+    WDL_LAUNCH_CHECK(ctx);
+  } else {
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(B.atoms64, atoms, KN * 8, cudaMemcpyDeviceToDevice, s));
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(B.lam64, weights, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  k_cast<float><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.atoms64, B.atoms, KN);
+  WDL_LAUNCH_CHECK(ctx);
+  k_cast<float><<<1, 256, 0, s>>>(B.lam64, B.lam, (size_t)P * K);
+  WDL_LAUNCH_CHECK(ctx);
+  if (b_init) {
+    k_cast<float><<<launch_cfg(ctx, PKN), 256, 0, s>>>(b_init, B.b0, PKN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  return WDL_OK;
+}
+
+SkArgs fused_args(const FusedBufs& B, int P, int K, int L, int loss_type, const double* obs,
+                  bool fwd_only) {
+  SkArgs a{};
+  a.P = P;
+  a.K = K;
+  a.L = L;
+  a.loss_type = loss_type;
+  a.fwd_only = fwd_only ? 1 : 0;
+  a.atoms = B.atoms;
+  a.lam = B.lam;
+  a.obs = obs;
+  a.b0 = B.b0;
+  a.cb = B.cb;
+  a.phi = B.phi;
+  a.acc = B.acc;
+  a.nb = B.nb;
+  a.gwb = B.gwb;
+  a.v = B.v;
+  a.r = B.r;
+  a.gdic = B.gdic;
+  a.dot = B.dot;
+  a.loss = B.loss;
+  a.sync = B.sync;
+  return a;
+}
+
+int gradient_both_fused(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                        const double* weights, const double* observed, const double* b_init,
+                        double* result_la, double* result_dic, double* bary_out, double* loss_out,
+                        double* b_last, cudaStream_t s, bool normalise) {
+  const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
+  int rc;
+  if ((rc = ensure_arena(ctx, fused_bytes(P, K, L, N, b_init != nullptr, false)))) return rc;
+  ctx->arena.reset();
+  FusedBufs B;
+  B.layout(ctx->arena, P, K, L, N, b_init != nullptr, false);
+  if ((rc = prepare_fused(ctx, B, P, K, atoms, weights, b_init, normalise, s))) return rc;
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.v, 0, PKN * 4, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.r, 0, PKN * 4, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, PKN * 4, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.dot, 0, (size_t)P * K * 8, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.acc, 0, (size_t)L * PN * 4, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.nb, 0, 2 * PN * 4, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gwb, 0, 2 * PN * 4, s));
+  SkArgs a = fused_args(B, P, K, L, loss_type, observed, false);
+  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
+  k_sum_over_p_f32<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
+  WDL_LAUNCH_CHECK(ctx);
+  const float* acc_L = B.acc + (size_t)(L - 1) * PN;
+  if (bary_out) {
+    k_exp_to_double<<<launch_cfg(ctx, PN), 256, 0, s>>>(acc_L, bary_out, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if (loss_out) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(loss_out, B.loss, (size_t)P * 8, cudaMemcpyDeviceToDevice, s));
+  if (b_last) {
+    k_b_last<<<launch_cfg(ctx, PKN), 256, 0, s>>>(acc_L, B.phi + (size_t)(L - 1) * PKN, b_last, K, N, PKN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  ctx->fused_sync = B.sync;
+  return WDL_OK;
+}
+
+int barycenter_fused(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
+                     double* bary_out, cudaStream_t s) {
+  const size_t N = ctx->N, PN = (size_t)P * N;
+  int rc;
+  if ((rc = ensure_arena(ctx, fused_bytes(P, K, L, N, false, true)))) return rc;
+  ctx->arena.reset();
+  FusedBufs B;
+  B.layout(ctx->arena, P, K, L, N, false, true);
+  if ((rc = prepare_fused(ctx, B, P, K, atoms, weights, nullptr, true, s))) return rc;
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.acc, 0, 2 * PN * 4, s));
+  SkArgs a = fused_args(B, P, K, L, WDL_LOSS_QUADRATIC, nullptr, true);
+  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
+  k_exp_to_double<<<launch_cfg(ctx, PN), 256, 0, s>>>(B.acc + (size_t)((L - 1) & 1) * PN, bary_out, PN);
+  WDL_LAUNCH_CHECK(ctx);
+  ctx->fused_sync = B.sync;
+  return WDL_OK;
+}
+
 bool use_fp64(const wdl_ctx* ctx) { return ctx->precision == WDL_FP64; }
 
 }  // namespace
 
 size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L) {
   const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
+  if (ctx->tc && !log_domain) {
+    const size_t a = fused_bytes(P, K, L, ctx->N, true, false);
+    const size_t b = eval_bytes_t<float>(P, K, L, ctx->N, false, true);  // Wasserstein loss runs unfused
+    return a > b ? a : b;
+  }
   return use_fp64(ctx) ? eval_bytes_t<double>(P, K, L, ctx->N, log_domain, true)
                        : eval_bytes_t<float>(P, K, L, ctx->N, log_domain, true);
 }
 
 size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K) {
+  if (ctx->tc && ctx->domain == WDL_DOMAIN_KERNEL) return fused_bytes(P, K, 2, ctx->N, false, true);
   const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
   const size_t t = use_fp64(ctx) ? 8 : 4;
   return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 16 * 256;
@@ -724,6 +898,9 @@ int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
                       const double* weights, const double* observed, const double* b_init,
                       double* result_la, double* result_dic, double* bary, double* loss,
                       double* b_last, cudaStream_t s, bool normalise) {
+  if (use_fused(ctx, loss_type))
+    return gradient_both_fused(ctx, P, K, L, loss_type, atoms, weights, observed, b_init, result_la,
+                               result_dic, bary, loss, b_last, s, normalise);
   if (use_fp64(ctx))
     return gradient_both_t<double>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
                                    result_la, result_dic, bary, loss, b_last, s, normalise);
@@ -733,6 +910,7 @@ int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
 
 int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
                    double* bary, cudaStream_t s) {
+  if (use_fused(ctx, WDL_LOSS_QUADRATIC)) return barycenter_fused(ctx, P, K, L, atoms, weights, bary, s);
   if (use_fp64(ctx)) return barycenter_t<double>(ctx, P, K, L, atoms, weights, bary, s);
   return barycenter_t<float>(ctx, P, K, L, atoms, weights, bary, s);
 }

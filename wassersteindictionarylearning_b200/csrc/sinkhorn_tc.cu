@@ -1,0 +1,609 @@
+// Persistent, dependency-driven tensor-core kernel for the whole Sinkhorn
+// forward pass, loss and reverse pass of P histograms (grid sides <= 128,
+// kernel domain, TF32 or split-BF16 operators, FP32 scalings and tape).
+//
+// Work items, claimed in order from one atomic counter by 2 warpgroups per CTA:
+//   FWD (it, p, k), it = 1..L          (cpp/inverseWasserstein.h:565-593)
+//     X1 = b[it-1] = bary[it-1]/phi[it-1] (b[0] = ones or the warm start)
+//     cb = G*X1 (stored), X2 = p_k/cb, phi[it] = G*X2 (stored)
+//   DICT (s, p, k), s = L..1           (:602-629)
+//     X1 = (lambda n - v) * b[s]; c = G*X1; gdic += c/cb[s-1];
+//     X2 = -p c/cb[s-1]^2; v = (G*X2)/phi[s-1]          (s = 1 stops after gdic)
+//   WGT (s, p, k), s = L..1            (:635-673)
+//     dot += sum log(phi[s]) gw;  X1 = (lambda gw - r)/phi[s];
+//     X2 = (G*X1)(-p/cb[s-1]^2); r = (G*X2) b[s-1]       (s = 1 stops after dot)
+// The cross-atom reductions are accumulated by the producing epilogues with
+// vector red.global.add into L2-resident buffers: FWD adds lambda_k
+// safe_log(phi_k) into acc[it][p] (bary[it] = exp(acc)), DICT adds v into
+// n[p] and WGT adds r into gw[p] (double-buffered by step parity).  An atomic
+// count per histogram detects the item that completes a group; it publishes a
+// per-histogram release flag (after the last forward iteration it also forms
+// the loss and the reverse-pass start n = g, gw = g*bary; in the reverse pass
+// it clears the message buffer the next step accumulates into).  Consumers wait
+// on the flags with a bounded acquire spin; an item only waits on items claimed
+// before it, so progress never depends on all CTAs being resident.  The float
+// atomics make the summation order of the K terms run-dependent (results are
+// reproducible to FP32 rounding, not bitwise).
+//
+// Each item runs two separable convolutions.  The first is in "column form"
+// (TMEM lane = x: the operand is staged from row-major global data and the
+// result is read back as columns), the second in "row form" (lane = y): the
+// column-form result, after the elementwise step, is exactly the row form's
+// K-major operand, so every SMEM write is a whole 16-byte chunk and every
+// global access of the epilogue is a contiguous row segment.
+#include "tc_common.cuh"
+#include "wdl_math.cuh"
+
+namespace wdl {
+
+namespace {
+using namespace tc;
+
+constexpr uint64_t kDepWaitNs = 4000000000ull;  // bound on a dependency wait
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ bool wait_ge(const int* flag, int target) {
+  if (ld_acquire(flag) >= target) return true;
+  const uint64_t t0 = ptx::globaltimer_ns();
+  while (true) {
+    __nanosleep(100);
+    if (ld_acquire(flag) >= target) return true;
+    if (ptx::globaltimer_ns() - t0 > kDepWaitNs) return false;
+  }
+}
+
+
+
+constexpr int kSt = 256;   // threads of one image stream (8 warps)
+constexpr int kWarps = kSt / 32;
+
+// Fast intrinsics for the tensor-core precisions: the operators themselves
+// round to TF32 or split BF16, so the elementwise steps use the hardware
+// reciprocal, exp2 and log2 (relative error ~1e-7, far below the operator's).
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float frcp(float b) { return __fdividef(1.0f, b); }
+
+// Stream-wide sum of a double (result valid in every thread of the stream).
+__device__ __forceinline__ double st_sum(double v, double* scratch, int st, int t) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((t & 31) == 0) scratch[st * kWarps + (t >> 5)] = v;
+  bar_sync(st, kSt);
+  double tot = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) tot += scratch[st * kWarps + w];
+  bar_sync(st, kSt);
+  return tot;
+}
+
+struct Geo {
+  int W, H, Wp, Hp;
+  uint32_t cpr, cpr_magic;  // operand chunks per row, ceil(2^32 / cpr)
+  bool vec;
+};
+
+// Stage the column-form operand X1(i, x) = f(in_0..in_{NIN-1} at (i, x)) for
+// rows i < Hp, x < Wp (zero outside the H x W image).  UNR chunks of loads are
+// issued before any is consumed.  f may accumulate side sums (captured by
+// reference); it is only called for pixels inside the image.
+template <bool SPLIT, int NIN, class F>
+__device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
+                                           F f, const Geo& g, int t) {
+  constexpr int CE = SPLIT ? 8 : 4;
+  constexpr int UNR = NIN > 2 ? 1 : 2;
+  const int total = g.Hp * (int)g.cpr;
+  for (int base = t; base < total; base += kSt * UNR) {
+    float in[UNR][NIN > 0 ? NIN : 1][CE];
+    int iu[UNR], xu[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int c = base + u * kSt;
+      const int i = (int)__umulhi((uint32_t)c, g.cpr_magic);
+      const int x0 = (c - i * (int)g.cpr) * CE;
+      iu[u] = i;
+      xu[u] = x0;
+      const bool row_ok = c < total && i < g.H;
+#pragma unroll
+      for (int a = 0; a < NIN; ++a) {
+        const float* row = src[a] + (size_t)i * g.W;
+        if (row_ok && g.vec && x0 + CE <= g.W) {
+#pragma unroll
+          for (int q = 0; q < CE; q += 4) {
+            const float4 f4 = __ldcg(reinterpret_cast<const float4*>(row + x0 + q));
+            in[u][a][q] = f4.x; in[u][a][q + 1] = f4.y; in[u][a][q + 2] = f4.z; in[u][a][q + 3] = f4.w;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < CE; ++q) in[u][a][q] = (row_ok && x0 + q < g.W) ? __ldcg(row + x0 + q) : 0.f;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      if (base + u * kSt >= total) break;
+      const int i = iu[u], x0 = xu[u];
+      float out[CE];
+#pragma unroll
+      for (int q = 0; q < CE; ++q) {
+        float av[NIN > 0 ? NIN : 1];
+#pragma unroll
+        for (int s = 0; s < NIN; ++s) av[s] = in[u][s][q];
+        out[q] = (i < g.H && x0 + q < g.W) ? f(av) : 0.f;
+      }
+      put_chunk<SPLIT>(tile, i, x0, out);
+    }
+  }
+}
+
+struct Ctl {
+  uint8_t* tile;
+  uint32_t g_a, x_a, bar_a, d1, d2, lane_base;
+  int st, t, lane_row, half;
+  uint32_t phase;
+};
+
+// Separable convolution of the operand tile: MMA1 (A = G, B = tile rows n, K =
+// K1) -> D1 -> restaged as the A operand (row = this thread's lane; warps w and
+// w+4 of the stream take alternate 16-column chunks of the same lanes) -> MMA2
+// (B = G) -> D2.  Column form: K1 = Wp, N1 = Hp; row form: K1 = Hp, N1 = Wp.
+template <bool SPLIT>
+__device__ bool gemm_pair(Ctl& c, int K1, int N1) {
+  ptx::tc_fence_before();
+  ptx::fence_proxy_async_smem();
+  bar_sync(c.st, kSt);
+  if (c.t == 0) {
+    ptx::tc_fence_after();
+    issue_gemm<SPLIT>(c.d1, c.g_a, c.x_a, K1, N1);
+    ptx::mma_commit(c.bar_a);
+  }
+  bool ok = bar_all(ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
+  c.phase ^= 1;
+  ptx::tc_fence_after();
+  for (int c0 = 16 * c.half; c0 < N1; c0 += 32) {
+    float v[16];
+    ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, v);
+    ptx::tmem_ld_wait();
+    put16<SPLIT>(c.tile, c.lane_row, c0, v);
+  }
+  ptx::tc_fence_before();
+  ptx::fence_proxy_async_smem();
+  bar_sync(c.st, kSt);
+  if (c.t == 0) {
+    ptx::tc_fence_after();
+    issue_gemm<SPLIT>(c.d2, c.x_a, c.g_a, N1, N1);
+    ptx::mma_commit(c.bar_a);
+  }
+  ok = bar_all(ok && ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
+  c.phase ^= 1;
+  ptx::tc_fence_after();
+  return ok;
+}
+
+// Column-form result D2[x][i] (x = this thread's lane): Y(i, x) for rows i in
+// chunks of 16.  For each chunk the NIN inputs at the 16 pixels idx = i*W + x
+// are loaded first (all loads in flight together), then m(idx, y, in) consumes
+// them (it may store) and returns the next operand's value, written as row x
+// (K = i) of the tile when stage_next.
+template <bool SPLIT, int NIN, class M>
+__device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
+                                            bool stage_next) {
+  const int x = c.lane_row;
+  for (int c0 = 16 * c.half; c0 < g.Hp; c0 += 32) {
+    float in[NIN][16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int i = c0 + t;
+      const bool ok = x < g.W && i < g.H;
+#pragma unroll
+      for (int q = 0; q < NIN; ++q) in[q][t] = ok ? __ldcg(src[q] + (size_t)i * g.W + x) : 1.f;
+    }
+    float y[16];
+    ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
+    ptx::tmem_ld_wait();
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int i = c0 + t;
+      float iv[NIN];
+#pragma unroll
+      for (int q = 0; q < NIN; ++q) iv[q] = in[q][t];
+      y[t] = (x < g.W && i < g.H) ? m((size_t)i * g.W + x, y[t], iv) : 0.f;
+    }
+    if (stage_next) put16<SPLIT>(c.tile, x, c0, y);
+  }
+}
+
+__device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
+               "f"(d)
+               : "memory");
+}
+__device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x) : (float)kLogEpsilon; }
+
+// Row-form result D2[i][x] (i = this thread's lane) with an accumulating
+// epilogue.  Per chunk of 16 columns the NIN inputs are loaded first (16-byte
+// vectors where rows are aligned); e(idx, y, in) may store and returns the
+// value added into acc[idx] (one 16-byte red per 4 pixels).
+template <int NIN, class E>
+__device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
+                                             float* acc, E e) {
+  const int i = c.lane_row;
+  for (int c0 = 16 * c.half; c0 < g.Wp; c0 += 32) {
+    const size_t row = (size_t)i * g.W;
+    const bool full = g.vec && c0 + 16 <= g.W && i < g.H;
+    float in[NIN > 0 ? NIN : 1][16];
+#pragma unroll
+    for (int q = 0; q < NIN; ++q) {
+      if (full) {
+#pragma unroll
+        for (int v4 = 0; v4 < 16; v4 += 4) {
+          const float4 f = __ldcg(reinterpret_cast<const float4*>(src[q] + row + c0 + v4));
+          in[q][v4] = f.x; in[q][v4 + 1] = f.y; in[q][v4 + 2] = f.z; in[q][v4 + 3] = f.w;
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+          in[q][t] = (i < g.H && c0 + t < g.W) ? __ldcg(src[q] + row + c0 + t) : 1.f;
+      }
+    }
+    float y[16];
+    ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
+    ptx::tmem_ld_wait();
+    if (i >= g.H) continue;
+    float out[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      float iv[NIN > 0 ? NIN : 1];
+#pragma unroll
+      for (int q = 0; q < NIN; ++q) iv[q] = in[q][t];
+      out[t] = (c0 + t < g.W) ? e(row + c0 + t, y[t], iv) : 0.f;
+    }
+    if (full) {
+#pragma unroll
+      for (int q = 0; q < 16; q += 4) red_add4(acc + row + c0 + q, out[q], out[q + 1], out[q + 2], out[q + 3]);
+    } else {
+#pragma unroll
+      for (int t = 0; t < 16; ++t)
+        if (c0 + t < g.W) atomicAdd(acc + row + c0 + t, out[t]);
+    }
+  }
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int st = warp / kWarps, t = tid % kSt, ws = warp % kWarps;
+  uint8_t* g_tile = base;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 3 * kTileBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + 3 * kTileBytes + 16);
+  int* s_int = reinterpret_cast<int*>(base + 3 * kTileBytes + 32);          // [2][4]
+  double* s_dbl = reinterpret_cast<double*>(base + 3 * kTileBytes + 64);    // [2][kWarps]
+
+  load_factor<SPLIT>(g_tile, a.G, a.Gn, tid, blockDim.x);
+  if (tid == 0) {
+    ptx::mbar_init(ptx::smem_addr(&bars[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[1]), 1);
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tmem_slot), 2 * kTmemCols);
+  ptx::fence_proxy_async_smem();
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+
+  Ctl c;
+  c.tile = base + (1 + st) * kTileBytes;
+  c.g_a = ptx::smem_addr(g_tile);
+  c.x_a = ptx::smem_addr(c.tile);
+  c.bar_a = ptx::smem_addr(&bars[st]);
+  c.d1 = *tmem_slot + (uint32_t)st * kTmemCols;
+  c.d2 = c.d1 + 128;
+  c.lane_base = (uint32_t)((ws & 3) * 32) << 16;
+  c.st = st;
+  c.t = t;
+  c.lane_row = (ws & 3) * 32 + lane;
+  c.half = ws >> 2;
+  c.phase = 0;
+
+  Geo g;
+  g.W = a.W;
+  g.H = a.H;
+  g.Wp = a.Wp;
+  g.Hp = a.Hp;
+  g.cpr = (uint32_t)(a.Wp / (SPLIT ? 8 : 4));
+  g.cpr_magic = (uint32_t)((0x100000000ull + g.cpr - 1) / g.cpr);
+  g.vec = a.vec != 0;
+  const int K = a.K, L = a.L, P = a.P;
+  const size_t N = a.N, PN = (size_t)P * N, PKN = (size_t)P * K * N;
+  const long long PK = (long long)P * K;
+  int* work = a.sync;
+  int* err = a.sync + 1;
+  int* done_fwd = a.sync + 2;
+  int* bary_ready = done_fwd + P;
+  int* done_bwd = bary_ready + P;
+  int* msg_ready = done_bwd + P;
+  // Tape slot of iteration it (1..L): all L kept for the reverse pass; two
+  // slots suffice for a forward-only run.
+  auto slot = [&](int it) -> size_t { return a.fwd_only ? (size_t)((it - 1) & 1) : (size_t)(it - 1); };
+
+  while (true) {
+    if (t == 0) s_int[st * 4] = atomicAdd(work, 1);
+    bar_sync(st, kSt);
+    const long long item = s_int[st * 4];
+    if (item >= a.total) break;
+    int type, step;  // type 0 = FWD, 1 = DICT, 2 = WGT
+    long long pk;
+    if (item < (long long)L * PK) {
+      type = 0;
+      step = (int)(item / PK) + 1;
+      pk = item % PK;
+    } else {
+      const long long j = item - (long long)L * PK;
+      step = L - (int)(j / (2 * PK));
+      const long long rem = j % (2 * PK);
+      pk = rem >> 1;
+      type = 1 + (int)(rem & 1);
+    }
+    const int p = (int)(pk / K), k = (int)(pk % K);
+    if (t == 0) {
+      bool ok = true;
+      if (type == 0) {
+        if (step > 1) ok = wait_ge(&bary_ready[p], step - 1);
+      } else {
+        ok = wait_ge(&msg_ready[p], L - step);
+      }
+      s_int[st * 4 + 1] = ok ? 1 : 0;
+    }
+    bar_sync(st, kSt);
+    if (!s_int[st * 4 + 1]) {
+      if (t == 0) atomicExch(err, WDL_ERR_TIMEOUT);
+      break;
+    }
+    const float lam = a.lam[pk];
+    const float* atom = a.atoms + (size_t)k * N;
+    bool ok = true;
+
+    if (type == 0) {  // ---------------- forward Bregman iteration
+      const int it = step;
+      float* cb_out = a.cb + slot(it) * PKN + pk * N;
+      float* phi_out = a.phi + slot(it) * PKN + pk * N;
+      float* acc_out = a.acc + slot(it) * PN + (size_t)p * N;
+      if (it == 1) {
+        if (a.b0) {
+          const float* src[1] = {a.b0 + pk * N};
+          stage_rows<SPLIT, 1>(c.tile, src, [](const float (&v)[1]) { return v[0]; }, g, t);
+        } else {
+          const float* src[1] = {atom};
+          stage_rows<SPLIT, 0>(c.tile, src, [](const float (&)[1]) { return 1.f; }, g, t);
+        }
+      } else {  // b[it-1] = exp(acc[it-1]) / phi[it-1]
+        const float* src[2] = {a.acc + slot(it - 1) * PN + (size_t)p * N,
+                               a.phi + slot(it - 1) * PKN + pk * N};
+        stage_rows<SPLIT, 2>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
+      }
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+      const bool keep_cb = !a.fwd_only;
+      const float* msrc[1] = {atom};
+      mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
+        if (keep_cb) __stcg(cb_out + idx, y);
+        return fdiv(in[0], y);
+      }, true);
+      ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+      const float* esrc[1] = {nullptr};
+      epi_rows_red<0>(c, g, esrc, acc_out, [&](size_t idx, float y, const float (&)[1]) {
+        __stcg(phi_out + idx, y);
+        return lam * safe_logf(y);
+      });
+    } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
+      const int s = step;
+      const float* src[4] = {a.nb + (size_t)(s & 1) * PN + (size_t)p * N, a.v + pk * N,
+                             a.acc + slot(s) * PN + (size_t)p * N, a.phi + slot(s) * PKN + pk * N};
+      stage_rows<SPLIT, 4>(c.tile, src,
+                           [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); },
+                           g, t);
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+      const float* cbp = a.cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
+      float* gd = a.gdic + pk * N;
+      const float* msrc[3] = {cbp, gd, atom};
+      mid_columns<SPLIT, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
+        const float rc = frcp(in[0]);
+        const float q = y * rc;
+        __stcg(gd + idx, in[1] + q);
+        return -in[2] * q * rc;
+      }, s > 1);
+      if (s > 1) {
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+        const float* php = a.phi + slot(s - 1) * PKN + pk * N;
+        float* vout = a.v + pk * N;
+        float* nout = a.nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
+        const float* esrc[1] = {php};
+        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float y, const float (&in)[1]) {
+          const float vv = fdiv(y, in[0]);
+          __stcg(vout + idx, vv);
+          return vv;
+        });
+      }
+    } else {  // ---------------- reverse pass, weight recursion
+      const int s = step;
+      const float* src[3] = {a.gwb + (size_t)(s & 1) * PN + (size_t)p * N, a.r + pk * N,
+                             a.phi + slot(s) * PKN + pk * N};
+      double dacc = 0;
+      stage_rows<SPLIT, 3>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
+        dacc += (double)__logf(v[2]) * (double)v[0];
+        return fdiv(lam * v[0] - v[1], v[2]);
+      }, g, t);
+      const double dsum = st_sum(dacc, s_dbl, st, t);
+      if (t == 0) atomicAdd(&a.dot[pk], dsum);
+      if (s > 1) {
+        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+        const float* cbp = a.cb + slot(s) * PKN + pk * N;
+        const float* msrc[2] = {cbp, atom};
+        mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
+          const float rc = frcp(in[0]);
+          return y * (-in[1] * rc * rc);
+        }, true);
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+        const float* php = a.phi + slot(s - 1) * PKN + pk * N;
+        const float* accp = a.acc + slot(s - 1) * PN + (size_t)p * N;
+        float* rout = a.r + pk * N;
+        float* gout = a.gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
+        const float* esrc[2] = {accp, php};
+        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float y, const float (&in)[2]) {
+          const float rr = y * fdiv(__expf(in[0]), in[1]);
+          __stcg(rout + idx, rr);
+          return rr;
+        });
+      }
+    }
+    if (!ok) {
+      if (t == 0) atomicExch(err, WDL_ERR_TIMEOUT);
+      break;
+    }
+
+    // Completion: the item that finishes a group publishes it.
+    bar_sync(st, kSt);
+    if (t == 0) {
+      __threadfence();
+      int fin;
+      if (type == 0) fin = atomicAdd(&done_fwd[p], 1) + 1 == step * K;
+      else fin = atomicAdd(&done_bwd[p], 1) + 1 == 2 * K * (L - step + 1);
+      s_int[st * 4 + 2] = fin;
+    }
+    bar_sync(st, kSt);
+    if (!s_int[st * 4 + 2]) continue;
+    __threadfence();
+    if (type == 0) {
+      const int it = step;
+      if (a.fwd_only && it >= 2) {
+        // acc[it-1] has been read by every item of iteration it: clear its slot,
+        // which iteration it+1 accumulates into.
+        float* z = a.acc + slot(it + 1) * PN + (size_t)p * N;
+        for (size_t j = t; j < N; j += kSt) __stcg(z + j, 0.f);
+      }
+      const bool last = it == L && !a.fwd_only;
+      if (last) {  // loss and its gradient (cpp/loss.h:19-90); messages for s = L
+        const float* accL = a.acc + slot(L) * PN + (size_t)p * N;
+        float* n0 = a.nb + (size_t)(L & 1) * PN + (size_t)p * N;
+        float* g0 = a.gwb + (size_t)(L & 1) * PN + (size_t)p * N;
+        double lacc = 0;
+        for (size_t j = t; j < N; j += kSt) {
+          const float bv = expf(__ldcg(accL + j));
+          const double o = a.obs[(size_t)p * N + j];
+          const float o32 = (float)o;
+          float gg;
+          if (a.loss_type == WDL_LOSS_TV) {
+            lacc += fabs((double)bv - o);
+            gg = (bv - o32) > 0.f ? 0.5f : -0.5f;
+          } else if (a.loss_type == WDL_LOSS_QUADRATIC) {
+            const double d = (double)bv - o;
+            lacc += d * d;
+            gg = 2.f * (bv - o32);
+          } else {
+            const double rr = (double)bv / o;
+            lacc += (double)bv * log(rr > kEpsilon ? rr : kEpsilon) - (double)bv + o;
+            const float q = bv / o32;
+            gg = q > 0.f ? logf(q) : (float)kLogEpsilon;
+          }
+          __stcg(n0 + j, gg);
+          __stcg(g0 + j, gg * bv);
+        }
+        const double tot = st_sum(lacc, s_dbl, st, t);
+        if (t == 0) a.loss[p] = a.loss_type == WDL_LOSS_TV ? 0.5 * tot : tot;
+      }
+      bar_sync(st, kSt);
+      if (t == 0) {
+        __threadfence();
+        st_release(&bary_ready[p], it);
+        if (last) st_release(&msg_ready[p], 0);
+      }
+    } else {
+      const int s = step;
+      if (s > 1) {  // the messages step s consumed are cleared for step s-2's sums
+        float* zn = a.nb + (size_t)(s & 1) * PN + (size_t)p * N;
+        float* zg = a.gwb + (size_t)(s & 1) * PN + (size_t)p * N;
+        for (size_t j = t; j < N; j += kSt) {
+          __stcg(zn + j, 0.f);
+          __stcg(zg + j, 0.f);
+        }
+      }
+      bar_sync(st, kSt);
+      if (t == 0) {
+        __threadfence();
+        st_release(&msg_ready[p], L - s + 1);
+      }
+    }
+  }
+  __syncthreads();
+  ptx::tc_fence_after();
+  if (warp == 0) ptx::tmem_dealloc(*tmem_slot, 2 * kTmemCols);
+}
+
+__global__ void k_sync_init(int* sync, int P) {
+  for (int i = threadIdx.x; i < 2 + 4 * P; i += blockDim.x) {
+    int v = 0;
+    if (i >= 2 + 3 * P) v = -1;  // msg_ready
+    sync[i] = v;
+  }
+}
+
+}  // namespace
+
+size_t sk_sync_ints(int P) { return 2 + 4 * (size_t)P; }
+
+int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
+  a.W = ctx->W;
+  a.H = ctx->H;
+  a.Wp = (a.W + 15) & ~15;
+  a.Hp = (a.H + 15) & ~15;
+  a.Gn = a.W >= a.H ? a.W : a.H;
+  a.G = ctx->G32[a.W >= a.H ? 0 : 1];
+  a.N = ctx->N;
+  a.vec = (a.W % 4) == 0;
+  const long long PK = (long long)a.P * a.K;
+  a.total = a.fwd_only ? (long long)a.L * PK : 3LL * a.L * PK;
+  k_sync_init<<<1, 256, 0, s>>>(a.sync, a.P);
+  WDL_LAUNCH_CHECK(ctx);
+  const size_t smem = 3 * tc::kTileBytes + 1024 + 256;
+  const bool split = ctx->precision == WDL_SPLIT_BF16;
+  if (split)
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  else
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long streams = (a.total + 1) / 2;
+  const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
+  if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
+  if (split) sinkhorn_tc_kernel<true><<<grid, 2 * kSt, smem, s>>>(a);
+  else sinkhorn_tc_kernel<false><<<grid, 2 * kSt, smem, s>>>(a);
+  WDL_LAUNCH_CHECK(ctx);
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->ev_b, s);
+    cudaEventSynchronize(ctx->ev_b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b);
+    ctx->conv_ms += ms;
+    ctx->conv_launches += 1;
+    // operator applications: 2 per FWD item, 2 per reverse item with s > 1,
+    // 1 per dictionary item at s = 1
+    const double convs = a.fwd_only ? 2.0 * a.L * PK : 2.0 * a.L * PK + 4.0 * (a.L - 1) * PK + PK;
+    ctx->conv_images += convs;
+  }
+  return WDL_OK;
+}
+
+// Status word of the fused kernel (sync[1]); cleared when read.
+int sinkhorn_tc_status(wdl_ctx* ctx, int* sync_dev) {
+  int h = 0;
+  WDL_CUDA_TRY(ctx, cudaMemcpy(&h, sync_dev + 1, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h != 0) return set_error(ctx, h, "fused tensor-core kernel: a bounded wait timed out");
+  return WDL_OK;
+}
+
+}  // namespace wdl

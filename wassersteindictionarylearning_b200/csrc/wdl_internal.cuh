@@ -75,6 +75,7 @@ struct wdl_ctx {
   wdl::Arena arena;  // compute workspace (tape, scratch)
   wdl::Arena io;     // staging of the host-pointer calls
   wdl::TcResources* tc = nullptr;
+  int* fused_sync = nullptr;  // status block of the last fused-kernel launch (in the arena)
 
   std::string last_error;
   long long launches = 0;
@@ -168,6 +169,29 @@ void tc_free(wdl_ctx* ctx);
 // wait gives up (WDL_ERR_TIMEOUT); WDL_OK otherwise.
 int tc_check_status(wdl_ctx* ctx);
 bool tc_supported(const wdl_ctx* ctx);
+
+// Fused persistent tensor-core Sinkhorn kernel (sinkhorn_tc.cu).
+struct SkArgs {
+  int P, K, L, W, H, Wp, Hp, Gn, loss_type, fwd_only, vec;
+  size_t N;
+  const float* G;
+  const float* atoms;    // [K][N]
+  const float* lam;      // [P][K]
+  const double* obs;     // [P][N]
+  const float* b0;       // [P][K][N] or null (ones)
+  float* cb;             // [slots][P][K][N]   conv_b tape
+  float* phi;            // [slots][P][K][N]   phi tape
+  float* acc;            // [slots][P][N]      sum_k lambda_k safe_log(phi_k): bary = exp(acc)
+  float *nb, *gwb;       // [2][P][N]          reverse-pass messages, by step parity
+  float *v, *r, *gdic;   // [P][K][N]
+  double* dot;           // [P][K]
+  double* loss;          // [P]
+  int* sync;             // work, err, done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P]
+  long long total;
+};
+size_t sk_sync_ints(int P);
+int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s);
+int sinkhorn_tc_status(wdl_ctx* ctx, int* sync_dev);
 
 // Hot path entry points (sinkhorn.cu); all pointers are device pointers.
 int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
