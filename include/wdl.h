@@ -149,11 +149,18 @@ int wdl_convolve_device(wdl_ctx* ctx, const double* u, double* out, int nvectors
 
 /* ---- Instrumentation ------------------------------------------------------------
  * Kernel launches issued by this context since creation (every kernel of this
- * library counts one), and the last call's time in the dominant convolution
- * kernel as measured with CUDA events on the launching stream (0 unless
- * wdl_set_profiling(ctx, 1)). */
+ * library counts one), and the time in the dominant kernel (the separable
+ * operator, or the fused Sinkhorn kernel on the tensor-core path) measured with
+ * CUDA events on the launching stream since profiling was switched on
+ * (level >= 1; the events synchronise each launch).  Level 2 also records a
+ * device-side phase trace of the fused kernel: wdl_phase_trace returns 27
+ * values, for item types forward / dictionary / weights, 8 accumulated phase
+ * times in ns (claim, dependency wait, prologue, first operator, mid step,
+ * second operator, epilogue, completion) and the item count.  (The reference
+ * only times whole L-BFGS iterations, cpp/chrono.h:52-78.) */
 long long wdl_launch_count(const wdl_ctx* ctx);
-int wdl_set_profiling(wdl_ctx* ctx, int on);
+int wdl_set_profiling(wdl_ctx* ctx, int level);
+int wdl_phase_trace(wdl_ctx* ctx, double* out27);
 int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launches,
                      double* conv_images);
 

@@ -71,6 +71,7 @@ SIGNATURES = {
     "wdl_launch_count": ([_vp], C.c_longlong),
     "wdl_set_profiling": ([_vp, C.c_int], C.c_int),
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),
+    "wdl_phase_trace": ([_vp, _dp], C.c_int),
 }
 
 _LIB = None

@@ -248,6 +248,7 @@ int wdl_destroy(wdl_ctx* ctx) {
     if (ctx->G32[a]) cudaFree(ctx->G32[a]);
   }
   if (ctx->arena.ptr) cudaFree(ctx->arena.ptr);
+  if (ctx->d_trace) cudaFree(ctx->d_trace);
   if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
   if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -271,9 +272,21 @@ long long wdl_launch_count(const wdl_ctx* ctx) { return ctx ? ctx->launches : -1
 int wdl_set_profiling(wdl_ctx* ctx, int on) {
   if (!ctx) return WDL_ERR_INVALID_ARG;
   ctx->profiling = on != 0;
+  ctx->trace_level = on;
   ctx->conv_ms = 0;
   ctx->conv_launches = 0;
   ctx->conv_images = 0;
+  return WDL_OK;
+}
+
+int wdl_phase_trace(wdl_ctx* ctx, double* out27) {
+  if (!ctx || !out27) return WDL_ERR_INVALID_ARG;
+  for (int i = 0; i < 27; ++i) out27[i] = 0;
+  if (!ctx->d_trace) return WDL_OK;
+  unsigned long long h[27];
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  WDL_CUDA_TRY(ctx, cudaMemcpy(h, ctx->d_trace, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < 27; ++i) out27[i] = (double)h[i];
   return WDL_OK;
 }
 

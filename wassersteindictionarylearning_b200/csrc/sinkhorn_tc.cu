@@ -82,6 +82,31 @@ __device__ __forceinline__ double st_sum(double v, double* scratch, int st, int 
   return tot;
 }
 
+// Pulls an image's 128-byte lines into L2 ahead of use (no registers, no wait).
+__device__ __forceinline__ void prefetch_l2(const float* p, size_t n, int t) {
+  for (size_t off = (size_t)t * 32; off < n; off += (size_t)kSt * 32)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
+}
+
+// Phase trace (thread 0 of a stream; only when a trace buffer is given):
+// claim, dependency wait, prologue, first convolution, mid, second
+// convolution, epilogue, completion; slot 8 counts items.
+struct Trace {
+  unsigned long long* buf;
+  uint64_t last;
+  int type;
+  __device__ void start(unsigned long long* b, int t0) {
+    buf = t0 == 0 ? b : nullptr;
+    if (buf) last = ptx::globaltimer_ns();
+  }
+  __device__ void mark(int phase) {
+    if (!buf) return;
+    const uint64_t now = ptx::globaltimer_ns();
+    atomicAdd(&buf[type * 9 + phase], (unsigned long long)(now - last));
+    last = now;
+  }
+};
+
 struct Geo {
   int W, H, Wp, Hp;
   uint32_t cpr, cpr_magic;  // operand chunks per row, ceil(2^32 / cpr)
@@ -226,51 +251,79 @@ __device__ __forceinline__ void red_add4(float* p, float a, float b, float c, fl
 __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x) : (float)kLogEpsilon; }
 
 // Row-form result D2[i][x] (i = this thread's lane) with an accumulating
-// epilogue.  Per chunk of 16 columns the NIN inputs are loaded first (16-byte
-// vectors where rows are aligned); e(idx, y, in) may store and returns the
-// value added into acc[idx] (one 16-byte red per 4 pixels).
+// epilogue.  The result is first staged in the (now free) operand tile as a
+// row-major FP32 image (512-byte rows, 16-byte chunk j of row i at position
+// j ^ (i % 8)), then the stream walks it row by row: 32 threads x 16 bytes
+// cover one row, so every global load, store and red is a contiguous 512-byte
+// row.  e(idx, y4, in4) gets 4 consecutive pixels, may store, and returns the
+// 4 values added into acc[idx..idx+3].
 template <int NIN, class E>
 __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
                                              float* acc, E e) {
-  const int i = c.lane_row;
-  for (int c0 = 16 * c.half; c0 < g.Wp; c0 += 32) {
-    const size_t row = (size_t)i * g.W;
-    const bool full = g.vec && c0 + 16 <= g.W && i < g.H;
-    float in[NIN > 0 ? NIN : 1][16];
+  {
+    const int i = c.lane_row;
+    uint8_t* rowp = c.tile + (size_t)i * 512;
+    for (int c0 = 16 * c.half; c0 < g.Wp; c0 += 32) {
+      float y[16];
+      ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
+      ptx::tmem_ld_wait();
 #pragma unroll
-    for (int q = 0; q < NIN; ++q) {
-      if (full) {
-#pragma unroll
-        for (int v4 = 0; v4 < 16; v4 += 4) {
-          const float4 f = __ldcg(reinterpret_cast<const float4*>(src[q] + row + c0 + v4));
-          in[q][v4] = f.x; in[q][v4 + 1] = f.y; in[q][v4 + 2] = f.z; in[q][v4 + 3] = f.w;
-        }
-      } else {
-#pragma unroll
-        for (int t = 0; t < 16; ++t)
-          in[q][t] = (i < g.H && c0 + t < g.W) ? __ldcg(src[q] + row + c0 + t) : 1.f;
+      for (int q = 0; q < 4; ++q) {
+        const int j = (c0 >> 2) + q;
+        *reinterpret_cast<float4*>(rowp + ((j ^ (i & 7)) << 4)) =
+            make_float4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
       }
     }
-    float y[16];
-    ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
-    ptx::tmem_ld_wait();
-    if (i >= g.H) continue;
-    float out[16];
+  }
+  bar_sync(c.st, kSt);
+  const int j = c.t & 31;  // 16-byte chunk of the row
+  const int x0 = 4 * j;
+  constexpr int U = 2;
+  for (int i0 = c.t >> 5; i0 < g.H; i0 += kWarps * U) {
+    float4 y4[U];
+    float in[U][NIN > 0 ? NIN : 1][4];
 #pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      float iv[NIN > 0 ? NIN : 1];
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * kWarps;
+      const bool okr = i < g.H && x0 < g.W;
+      y4[u] = okr ? *reinterpret_cast<const float4*>(c.tile + (size_t)i * 512 + ((j ^ (i & 7)) << 4))
+                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      const size_t idx = (size_t)i * g.W + x0;
 #pragma unroll
-      for (int q = 0; q < NIN; ++q) iv[q] = in[q][t];
-      out[t] = (c0 + t < g.W) ? e(row + c0 + t, y[t], iv) : 0.f;
+      for (int q = 0; q < NIN; ++q) {
+        if (okr && g.vec) {
+          const float4 f = __ldcg(reinterpret_cast<const float4*>(src[q] + idx));
+          in[u][q][0] = f.x; in[u][q][1] = f.y; in[u][q][2] = f.z; in[u][q][3] = f.w;
+        } else {
+#pragma unroll
+          for (int r = 0; r < 4; ++r) in[u][q][r] = (okr && x0 + r < g.W) ? __ldcg(src[q] + idx + r) : 1.f;
+        }
+      }
     }
-    if (full) {
 #pragma unroll
-      for (int q = 0; q < 16; q += 4) red_add4(acc + row + c0 + q, out[q], out[q + 1], out[q + 2], out[q + 3]);
-    } else {
-#pragma unroll
-      for (int t = 0; t < 16; ++t)
-        if (c0 + t < g.W) atomicAdd(acc + row + c0 + t, out[t]);
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * kWarps;
+      if (i >= g.H || x0 >= g.W) continue;
+      const size_t idx = (size_t)i * g.W + x0;
+      const int nv = g.W - x0 < 4 ? g.W - x0 : 4;
+      const float4 out = e(idx, y4[u], in[u], nv);
+      if (g.vec) {
+        red_add4(acc + idx, out.x, out.y, out.z, out.w);
+      } else {
+        const float o[4] = {out.x, out.y, out.z, out.w};
+        for (int r = 0; r < nv; ++r) atomicAdd(acc + idx + r, o[r]);
+      }
     }
+  }
+}
+
+// Stores 4 consecutive values (nv valid; 16-byte store when the row is aligned).
+__device__ __forceinline__ void st4(float* p, float4 v, int nv, bool vec) {
+  if (vec) {
+    __stcg(reinterpret_cast<float4*>(p), v);
+  } else {
+    const float o[4] = {v.x, v.y, v.z, v.w};
+    for (int r = 0; r < nv; ++r) __stcg(p + r, o[r]);
   }
 }
 
@@ -334,7 +387,10 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   // slots suffice for a forward-only run.
   auto slot = [&](int it) -> size_t { return a.fwd_only ? (size_t)((it - 1) & 1) : (size_t)(it - 1); };
 
+  Trace tr;
   while (true) {
+    tr.start(a.trace, t);
+    tr.type = 0;
     if (t == 0) s_int[st * 4] = atomicAdd(work, 1);
     bar_sync(st, kSt);
     const long long item = s_int[st * 4];
@@ -353,6 +409,34 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       type = 1 + (int)(rem & 1);
     }
     const int p = (int)(pk / K), k = (int)(pk % K);
+    tr.type = type;
+    {  // every array this item reads, requested into L2 up front
+      const size_t pkN = (size_t)pk * N, pN = (size_t)p * N;
+      if (type == 0) {
+        if (step > 1) {
+          prefetch_l2(a.acc + slot(step - 1) * PN + pN, N, t);
+          prefetch_l2(a.phi + slot(step - 1) * PKN + pkN, N, t);
+        } else if (a.b0) {
+          prefetch_l2(a.b0 + pkN, N, t);
+        }
+      } else {
+        const int s = step;
+        prefetch_l2(a.phi + slot(s) * PKN + pkN, N, t);
+        prefetch_l2(a.cb + slot(s) * PKN + pkN, N, t);
+        if (s > 1) prefetch_l2(a.phi + slot(s - 1) * PKN + pkN, N, t);
+        if (type == 1) {
+          prefetch_l2(a.nb + (size_t)(s & 1) * PN + pN, N, t);
+          prefetch_l2(a.v + pkN, N, t);
+          prefetch_l2(a.acc + slot(s) * PN + pN, N, t);
+          prefetch_l2(a.gdic + pkN, N, t);
+        } else {
+          prefetch_l2(a.gwb + (size_t)(s & 1) * PN + pN, N, t);
+          prefetch_l2(a.r + pkN, N, t);
+          if (s > 1) prefetch_l2(a.acc + slot(s - 1) * PN + pN, N, t);
+        }
+      }
+    }
+    tr.mark(0);
     if (t == 0) {
       bool ok = true;
       if (type == 0) {
@@ -367,6 +451,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       if (t == 0) atomicExch(err, WDL_ERR_TIMEOUT);
       break;
     }
+    tr.mark(1);
     const float lam = a.lam[pk];
     const float* atom = a.atoms + (size_t)k * N;
     bool ok = true;
@@ -389,19 +474,25 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
                                a.phi + slot(it - 1) * PKN + pk * N};
         stage_rows<SPLIT, 2>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
       }
+      tr.mark(2);
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+      tr.mark(3);
       const bool keep_cb = !a.fwd_only;
       const float* msrc[1] = {atom};
       mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
         if (keep_cb) __stcg(cb_out + idx, y);
         return fdiv(in[0], y);
       }, true);
+      tr.mark(4);
       ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+      tr.mark(5);
       const float* esrc[1] = {nullptr};
-      epi_rows_red<0>(c, g, esrc, acc_out, [&](size_t idx, float y, const float (&)[1]) {
-        __stcg(phi_out + idx, y);
-        return lam * safe_logf(y);
+      epi_rows_red<0>(c, g, esrc, acc_out, [&](size_t idx, float4 y, const float (&)[1][4], int nv) {
+        st4(phi_out + idx, y, nv, g.vec);
+        return make_float4(lam * safe_logf(y.x), lam * safe_logf(y.y), lam * safe_logf(y.z),
+                           lam * safe_logf(y.w));
       });
+      tr.mark(6);
     } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
       const int s = step;
       const float* src[4] = {a.nb + (size_t)(s & 1) * PN + (size_t)p * N, a.v + pk * N,
@@ -409,7 +500,9 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       stage_rows<SPLIT, 4>(c.tile, src,
                            [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); },
                            g, t);
+      tr.mark(2);
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+      tr.mark(3);
       const float* cbp = a.cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
       float* gd = a.gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
@@ -419,17 +512,21 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         __stcg(gd + idx, in[1] + q);
         return -in[2] * q * rc;
       }, s > 1);
+      tr.mark(4);
       if (s > 1) {
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+        tr.mark(5);
         const float* php = a.phi + slot(s - 1) * PKN + pk * N;
         float* vout = a.v + pk * N;
         float* nout = a.nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[1] = {php};
-        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float y, const float (&in)[1]) {
-          const float vv = fdiv(y, in[0]);
-          __stcg(vout + idx, vv);
+        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
+          const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
+                                        fdiv(y.w, in[0][3]));
+          st4(vout + idx, vv, nv, g.vec);
           return vv;
         });
+        tr.mark(6);
       }
     } else {  // ---------------- reverse pass, weight recursion
       const int s = step;
@@ -442,25 +539,33 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       }, g, t);
       const double dsum = st_sum(dacc, s_dbl, st, t);
       if (t == 0) atomicAdd(&a.dot[pk], dsum);
+      tr.mark(2);
       if (s > 1) {
         ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+        tr.mark(3);
         const float* cbp = a.cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
         mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
           return y * (-in[1] * rc * rc);
         }, true);
+        tr.mark(4);
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+        tr.mark(5);
         const float* php = a.phi + slot(s - 1) * PKN + pk * N;
         const float* accp = a.acc + slot(s - 1) * PN + (size_t)p * N;
         float* rout = a.r + pk * N;
         float* gout = a.gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[2] = {accp, php};
-        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float y, const float (&in)[2]) {
-          const float rr = y * fdiv(__expf(in[0]), in[1]);
-          __stcg(rout + idx, rr);
+        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
+          const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
+                                        y.y * fdiv(__expf(in[0][1]), in[1][1]),
+                                        y.z * fdiv(__expf(in[0][2]), in[1][2]),
+                                        y.w * fdiv(__expf(in[0][3]), in[1][3]));
+          st4(rout + idx, rr, nv, g.vec);
           return rr;
         });
+        tr.mark(6);
       }
     }
     if (!ok) {
@@ -478,7 +583,11 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       s_int[st * 4 + 2] = fin;
     }
     bar_sync(st, kSt);
-    if (!s_int[st * 4 + 2]) continue;
+    if (!s_int[st * 4 + 2]) {
+      tr.mark(7);
+      if (tr.buf) atomicAdd(&tr.buf[type * 9 + 8], 1ull);
+      continue;
+    }
     __threadfence();
     if (type == 0) {
       const int it = step;
@@ -540,6 +649,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         st_release(&msg_ready[p], L - s + 1);
       }
     }
+    tr.mark(7);
+    if (tr.buf) atomicAdd(&tr.buf[type * 9 + 8], 1ull);
   }
   __syncthreads();
   ptx::tc_fence_after();
@@ -580,6 +691,12 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
   const long long streams = (a.total + 1) / 2;
   const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
   if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
+  a.trace = nullptr;
+  if (ctx->trace_level >= 2) {
+    if (!ctx->d_trace) WDL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_trace, 27 * sizeof(unsigned long long)));
+    WDL_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_trace, 0, 27 * sizeof(unsigned long long), s));
+    a.trace = ctx->d_trace;
+  }
   if (split) sinkhorn_tc_kernel<true><<<grid, 2 * kSt, smem, s>>>(a);
   else sinkhorn_tc_kernel<false><<<grid, 2 * kSt, smem, s>>>(a);
   WDL_LAUNCH_CHECK(ctx);

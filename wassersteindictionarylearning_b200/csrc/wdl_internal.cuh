@@ -85,6 +85,8 @@ struct wdl_ctx {
   double conv_ms = 0;
   long long conv_launches = 0;
   double conv_images = 0;
+  int trace_level = 0;                    // 2: per-phase device trace of the fused kernel
+  unsigned long long* d_trace = nullptr;  // [27] accumulated ns / counts
 };
 
 namespace wdl {
@@ -187,6 +189,7 @@ struct SkArgs {
   double* dot;           // [P][K]
   double* loss;          // [P]
   int* sync;             // work, err, done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P]
+  unsigned long long* trace;  // [3 item types][8 phases + 1 count] ns, or null
   long long total;
 };
 size_t sk_sync_ints(int P);
