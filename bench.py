@@ -53,7 +53,7 @@ def parse():
 
 
 def default_precision():
-    return os.environ.get("WDL_BENCH_PRECISION", "fp32")
+    return os.environ.get("WDL_BENCH_PRECISION", "split_bf16")
 
 
 def dtype_name(precision):
