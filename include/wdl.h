@@ -147,6 +147,21 @@ int wdl_gradient_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, c
                              double* b_last, void* stream);
 int wdl_convolve_device(wdl_ctx* ctx, const double* u, double* out, int nvectors, void* stream);
 
+/* No counterpart in the reference (which has no device code).  The operator of
+ * wdl_convolve_device for callers that cannot allocate device memory while they
+ * run (hosts that reserve all memory at start-up, processes under a device
+ * memory cap or pool, code building a CUDA graph): it calls no cudaMalloc,
+ * cudaFree or other allocating routine, and takes its scratch from one fixed
+ * 32 MiB device array inside the library, which every GPU that loads the
+ * library holds until the process exits.  The caller passes device input and
+ * output.  3 * nvectors * N * (4 bytes, or 8 for WDL_FP64) rounded up must fit
+ * in the 32 MiB, otherwise WDL_ERR_INVALID_ARG (the message gives the limit).
+ * All calls share the array: calls that overlap on the GPU race, so serialise
+ * them.  The first call on each device looks up the array's device address;
+ * make that first call before any stream capture. */
+int wdl_convolve_device_noalloc(wdl_ctx* ctx, const double* u, double* out, int nvectors,
+                                void* stream);
+
 /* ---- Instrumentation ------------------------------------------------------------
  * Kernel launches issued by this context since creation (every kernel of this
  * library counts one), and the time in the dominant kernel (the separable

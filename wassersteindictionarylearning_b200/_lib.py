@@ -68,6 +68,7 @@ SIGNATURES = {
     "wdl_gradient_both_device": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp,
                                   _vp, _vp, _vp, _vp, _vp], C.c_int),
     "wdl_convolve_device": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
+    "wdl_convolve_device_noalloc": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
     "wdl_launch_count": ([_vp], C.c_longlong),
     "wdl_set_profiling": ([_vp, C.c_int], C.c_int),
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),
