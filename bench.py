@@ -194,6 +194,7 @@ def run_ours(args):
 
     import wassersteindictionarylearning_b200 as w
     from wassersteindictionarylearning_b200 import _lib
+    from wassersteindictionarylearning_b200.parallel import allreduce_atoms_and_loss
     from wassersteindictionarylearning_b200.synthetic import make_problem, to_variables
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -232,7 +233,6 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     sptr = C.c_void_p(stream.cuda_stream)
-    fg = torch.empty(K * N + 1, dtype=torch.float64, device=dev)
 
     def step():
         rc = L_.wdl_evaluate_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(x_d.data_ptr()),
@@ -241,11 +241,7 @@ def run_ours(args):
                                          None, None, None, sptr)
         _lib.check(rc, ctx)
         if world > 1:  # the path's one exchange: dictionary gradient + loss
-            fg[: K * N].copy_(g_d[PK:])
-            fg[K * N:].copy_(f_d)
-            dist.all_reduce(fg)
-            g_d[PK:].copy_(fg[: K * N])
-            f_d.copy_(fg[K * N:])
+            allreduce_atoms_and_loss(g_d, f_d, PK, dist)
 
     for _ in range(args.warmup):
         step()
@@ -326,10 +322,10 @@ def run_ours(args):
                                       None, None, None)
             _lib.check(rc, ctx)
             if world > 1:
-                fg[: K * N].copy_(gh[PK:].to(dev, non_blocking=False))
-                fg[K * N:] = float(fh[0])
-                dist.all_reduce(fg)
-                gh[PK:].copy_(fg[: K * N].cpu())
+                gd_, fd_ = gh.to(dev), fh.to(dev)
+                allreduce_atoms_and_loss(gd_, fd_, PK, dist)
+                gh[PK:].copy_(gd_[PK:].cpu())
+                fh.copy_(fd_.cpu())
         host_step()
         if world > 1:
             dist.barrier()
