@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--precision", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-rates", default="20,200")
+    ap.add_argument("--serve-requests", type=int, default=120)
     # Reduced sizes for profiler captures (the bench line itself uses the workload's).
     ap.add_argument("--P", type=int, default=None)
     ap.add_argument("--L", type=int, default=None)
@@ -341,6 +344,11 @@ def run_ours(args):
         d2h = (n + 1) * 8 + (K * N * 8 if world > 1 else 0)
         e2e = dict(value=units / el, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h)
 
+    serving = None
+    if rank == 0 and not args.no_serving:
+        serving = [run_serving(float(r), args.serve_requests, local)
+                   for r in args.serve_rates.split(",") if r]
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = time_cpu_reference(steps=1, warmup=0)
@@ -362,8 +370,32 @@ def run_ours(args):
                             l2=f"working set larger than L2: iterate store {tape_gb:.2f} GB per GPU",
                             objective=fval),
                 roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=int(gpu_launches),
-                clocks=clocks)
+                clocks=clocks, serving=serving)
     print(json.dumps(line), flush=True)
+
+
+def run_serving(rate, n, device):
+    """p50/p99 latency of a Poisson request stream through the serving loop:
+    half projection (fit 5 weights of a new histogram, L-BFGS) and half
+    barycenter requests, 2-D sides uniform in 64..256 and 20 % 48^3 volumes,
+    L = 50, gamma = 2, split-BF16 where the tensor-core operator applies."""
+    import time as _t
+
+    from wassersteindictionarylearning_b200.serving import (ServingEngine, latency_summary,
+                                                            poisson_requests)
+    arr = poisson_requests(rate, n, seed=11, K=5)
+    eng = ServingEngine(K=5, L=50, gamma=2.0, loss_type=2, precision="split_bf16",
+                        lbfgs_iterations=20, device=device)
+    t0 = _t.perf_counter()
+    done = eng.run(arr, timeout=240.0)
+    wall = _t.perf_counter() - t0
+    eng.close()
+    out = latency_summary(done)
+    out.update(offered_rate_req_s=rate, requests=n, wall_s=wall,
+               throughput_req_s=out["completed"] / wall,
+               mix="50% projection (20 L-BFGS iterations) / 50% barycenter; 2-D sides U[64,256], "
+                   "20% 48^3; L=50, gamma=2, K=5")
+    return out
 
 
 def main():

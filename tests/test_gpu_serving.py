@@ -1,0 +1,84 @@
+"""GPU: the continuous-batching serving loop.
+
+Each request's result is the same served alone and served inside a mixed
+stream (other shapes and kinds arriving while it runs): bitwise in FP64 (the
+FP64 path has no atomics), within tolerance on the split-BF16 path (whose
+cross-atom sums use float atomics).  Admission by iterate-store bytes: a request
+that can never fit is refused, the rest still complete; barycenter results match
+the oracle."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream(n, seed, sides=(32, 48, 64), frac_3d=0.2, cube=12, rate=400.0):
+    from wassersteindictionarylearning_b200.serving import poisson_requests
+    return poisson_requests(rate, n, seed=seed, K=3, frac_3d=frac_3d, sides=sides, cube=cube)
+
+
+def _engine(precision, **kw):
+    from wassersteindictionarylearning_b200.serving import ServingEngine
+    return ServingEngine(K=3, L=12, gamma=2.0, loss_type=2, precision=precision,
+                         lbfgs_iterations=8, **kw)
+
+
+@pytest.mark.parametrize("precision,tol_b,tol_w", [("fp64", 0.0, 0.0), ("split_bf16", 1e-5, 2e-3)])
+def test_alone_equals_mixed(precision, tol_b, tol_w):
+    import copy
+    arr = _stream(16, seed=3)
+    eng = _engine(precision)
+    done = {r.rid: r for r in eng.run(copy.deepcopy(arr))}
+    eng.close()
+    mixed = sorted(done.values(), key=lambda r: r.rid)
+    assert len(mixed) == 16 and all(r.status == 0 for r in mixed)
+    for i, (_, req) in enumerate(arr):
+        eng1 = _engine(precision)
+        alone = eng1.run([(0.0, copy.deepcopy(req))])[0]
+        eng1.close()
+        m = mixed[i]
+        assert m.kind == alone.kind and m.shape == alone.shape
+        if tol_b == 0.0:
+            assert np.array_equal(m.result, alone.result), (m.kind, m.shape)
+        elif m.kind == "barycenter":
+            assert rel(m.result, alone.result) < tol_b
+        else:
+            assert np.max(np.abs(m.result - alone.result)) < tol_w
+
+
+def test_barycenter_requests_match_oracle(oracle):
+    from wassersteindictionarylearning_b200.serving import BARYCENTER, Request
+    eng = _engine("fp64")
+    reqs = []
+    for i, shape in enumerate([(20, 16, 1), (20, 16, 1), (9, 8, 7)]):
+        w = np.array([0.2, 0.5, 0.3]) + 0.1 * i
+        reqs.append((0.0, Request(BARYCENTER, shape, weights=w / w.sum())))
+    done = sorted(eng.run(reqs), key=lambda r: r.rid)
+    for r in done:
+        W, H, D = r.shape
+        ref = oracle.barycenter(W, H, D, 2.0, 3, 12, eng.dictionary(r.shape), r.weights)
+        assert rel(r.result, ref) < 1e-10
+    eng.close()
+
+
+def test_admission_by_bytes():
+    from wassersteindictionarylearning_b200.serving import PROJECTION, Request
+    from wassersteindictionarylearning_b200.synthetic import blob_histograms
+    big = Request(PROJECTION, (64, 64, 1), observed=blob_histograms(1, 64, 64, seed=1)[0])
+    small = [Request(PROJECTION, (32, 32, 1), observed=blob_histograms(1, 32, 32, seed=2 + i)[0])
+             for i in range(3)]
+    probe = _engine("fp32")
+    b_small, b_big = probe.request_bytes(small[0]), probe.request_bytes(big)
+    probe.close()
+    assert b_big > 1.6 * b_small
+    eng = _engine("fp32", hbm_budget=1.5 * b_small)  # room for one small request at a time
+    done = eng.run([(0.0, big)] + [(0.0, s) for s in small])
+    st = {r.rid: r.status for r in done}
+    assert st[0] == -7                       # WDL_ERR_ADMISSION: never fits
+    assert all(st[i] == 0 for i in (1, 2, 3))  # served one after another
+    order = [r.rid for r in done if r.status == 0]
+    assert order == [1, 2, 3]
+    assert eng.admitted_bytes == 0
+    eng.close()

@@ -117,3 +117,23 @@ def test_lbfgs_cancel_on_nan():
     ret, _, _ = lb.lbfgs(np.zeros(3), ev, prog, lb.LbfgsParam(max_iterations=5))
     # NaN fails the sufficient-decrease test until the trial budget runs out
     assert ret in (lb.LBFGSERR_CANCELED, lb.LBFGSERR_MAXIMUMLINESEARCH)
+
+
+def test_resumable_lbfgs_matches_blocking_form():
+    from wassersteindictionarylearning_b200 import lbfgs as lb
+    A = np.diag(np.linspace(1.0, 30.0, 12))
+    b = np.linspace(-1, 1, 12)
+
+    def ev(x, step=0.0):
+        return 0.5 * x @ A @ x - b @ x, A @ x - b
+
+    p = lb.LbfgsParam(max_iterations=15)
+    r1, x1, f1 = lb.lbfgs(np.zeros(12), ev, None, p)
+    gen = lb.lbfgs_steps(np.zeros(12), p)
+    x = next(gen)
+    try:
+        while True:
+            x = gen.send(ev(x))
+    except StopIteration as e:
+        r2, x2, f2 = e.value
+    assert r1 == r2 and np.array_equal(x1, x2) and f1 == f2

@@ -49,6 +49,87 @@ Evaluate = Callable[[np.ndarray, float], tuple]        # (x, step) -> (f, g)
 Progress = Callable[[np.ndarray, np.ndarray, float, float, float, float, int, int], int]
 
 
+def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
+    """Resumable form: a generator that yields each point to evaluate and
+    receives (f, g) through send(); it returns (status, x, f) via StopIteration.
+    Same algorithm and constants as lbfgs() below (which drives it)."""
+    p = param or LbfgsParam()
+    x = np.array(x0, dtype=np.float64, copy=True)
+    n = x.size
+    f, g = yield x
+    g = np.asarray(g, dtype=np.float64)
+    d = -g
+    xnorm = max(float(np.linalg.norm(x)), 1.0)
+    gnorm = float(np.linalg.norm(g))
+    if gnorm / xnorm <= p.epsilon:
+        return LBFGS_ALREADY_MINIMIZED, x, f
+    step = 1.0 / float(np.sqrt(np.dot(d, d)))
+    s_hist = np.zeros((p.m, n))
+    y_hist = np.zeros((p.m, n))
+    ys_hist = np.zeros(p.m)
+    alpha = np.zeros(p.m)
+    k, end = 1, 0
+    while True:
+        xp, gp = x.copy(), g.copy()
+        # backtracking line search with the strong Wolfe test (lbfgs.c:772-867)
+        if step <= 0:
+            return LBFGSERR_INVALIDPARAMETERS, xp, f
+        dginit = float(np.dot(g, d))
+        if dginit > 0:
+            return LBFGSERR_INCREASEGRADIENT, xp, f
+        finit, dgtest, count = f, p.ftol * dginit, 0
+        while True:
+            x = xp + step * d
+            f, g = yield x
+            g = np.asarray(g, dtype=np.float64)
+            count += 1
+            if f > finit + step * dgtest:
+                width = 0.5
+            else:
+                dg = float(np.dot(g, d))
+                if dg < p.wolfe * dginit:
+                    width = 2.1
+                elif dg > -p.wolfe * dginit:
+                    width = 0.5
+                else:
+                    break
+            if step < p.min_step:
+                return LBFGSERR_MINIMUMSTEP, xp, f
+            if step > p.max_step:
+                return LBFGSERR_MAXIMUMSTEP, xp, f
+            if p.max_linesearch <= count:
+                return LBFGSERR_MAXIMUMLINESEARCH, xp, f
+            step *= width
+        xnorm = float(np.linalg.norm(x))
+        gnorm = float(np.linalg.norm(g))
+        if np.isnan(f):
+            return LBFGSERR_CANCELED, x, f
+        if gnorm / max(xnorm, 1.0) <= p.epsilon:
+            return LBFGS_SUCCESS, x, f
+        if p.max_iterations != 0 and p.max_iterations < k + 1:
+            return LBFGSERR_MAXIMUMITERATION, x, f
+        s_hist[end] = x - xp
+        y_hist[end] = g - gp
+        ys = float(np.dot(y_hist[end], s_hist[end]))
+        yy = float(np.dot(y_hist[end], y_hist[end]))
+        ys_hist[end] = ys
+        bound = min(p.m, k)
+        k += 1
+        end = (end + 1) % p.m
+        d = -g
+        j = end
+        for _ in range(bound):
+            j = (j + p.m - 1) % p.m
+            alpha[j] = float(np.dot(s_hist[j], d)) / ys_hist[j]
+            d = d - alpha[j] * y_hist[j]
+        d = d * (ys / yy)
+        for _ in range(bound):
+            beta = float(np.dot(y_hist[j], d)) / ys_hist[j]
+            d = d + (alpha[j] - beta) * s_hist[j]
+            j = (j + 1) % p.m
+        step = 1.0
+
+
 def _line_search(x, f, g, d, step, xp, evaluate, p: LbfgsParam):
     """Backtracking with the strong Wolfe conditions; returns (count or code, x, f, g, step)."""
     count = 0
