@@ -135,6 +135,33 @@ int wdl_evaluate_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double s
 int wdl_barycenter(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
                    double* bary);
 
+/* ---- Batched independent problems ----------------------------------------------
+ * Many independent problems in ONE persistent launch: each its own grid (2-D,
+ * sides up to the context's, which must be a WDL_TF32 / WDL_SPLIT_BF16 kernel-
+ * domain context of sides <= 128), atom count, iteration count, histogram count
+ * and mode; all share the context's gamma.  Per problem, with host pointers:
+ *   WDL_MODE_WEIGHTS     forward + weight recursion: result_la [P*K] (raw
+ *                        resultLa), loss [P]; the dictionary recursion is skipped
+ *                        (weight fitting / projection onto fixed atoms)
+ *   WDL_MODE_BOTH        compute_gradient_both: result_la, result_dic [K*N]
+ *                        (summed over P), loss
+ *   WDL_MODE_BARYCENTER  forward only: bary [P*N] (compute_barycenter)
+ * Any output pointer may be NULL.  No reference counterpart (the reference runs
+ * one problem at a time); each problem's results equal a separate
+ * wdl_gradient_both / wdl_barycenter call on its own grid. */
+enum { WDL_MODE_WEIGHTS = 0, WDL_MODE_BOTH = 1, WDL_MODE_BARYCENTER = 2 };
+typedef struct {
+  int W, H, K, L, P, loss_type, mode;
+  const double* atoms;     /* [K*N] */
+  const double* weights;   /* [P*K] */
+  const double* observed;  /* [P*N], unused for WDL_MODE_BARYCENTER */
+  double* result_la;       /* [P*K] or NULL */
+  double* result_dic;      /* [K*N] or NULL (WDL_MODE_BOTH) */
+  double* bary;            /* [P*N] or NULL */
+  double* loss;            /* [P] or NULL */
+} wdl_problem;
+int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* problems, int nproblems);
+
 /* ---- Device-resident forms (device pointers, stream as void*) ----------------
  * Same semantics as the host forms; no host<->device copies, no synchronisation.
  * f is a device double. */

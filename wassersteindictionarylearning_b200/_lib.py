@@ -29,6 +29,16 @@ ERRORS = {
 _dp = C.POINTER(C.c_double)
 _vp = C.c_void_p
 
+WDL_MODE_WEIGHTS, WDL_MODE_BOTH, WDL_MODE_BARYCENTER = 0, 1, 2
+
+
+class WdlProblem(C.Structure):
+    """struct wdl_problem of include/wdl.h."""
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("K", C.c_int), ("L", C.c_int), ("P", C.c_int),
+                ("loss_type", C.c_int), ("mode", C.c_int), ("atoms", _dp), ("weights", _dp),
+                ("observed", _dp), ("result_la", _dp), ("result_dic", _dp), ("bary", _dp),
+                ("loss", _dp)]
+
 
 class WdlError(RuntimeError):
     def __init__(self, code: int, detail: str):
@@ -69,6 +79,7 @@ SIGNATURES = {
                                   _vp, _vp, _vp, _vp, _vp], C.c_int),
     "wdl_convolve_device": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
     "wdl_convolve_device_noalloc": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
+    "wdl_batch_run": ([_vp, C.c_void_p, C.c_int], C.c_int),
     "wdl_launch_count": ([_vp], C.c_longlong),
     "wdl_set_profiling": ([_vp, C.c_int], C.c_int),
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),

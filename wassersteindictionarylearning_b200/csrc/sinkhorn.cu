@@ -731,7 +731,8 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
 struct FusedBufs {
   double *atoms64, *lam64, *dot, *loss;
   float *atoms, *lam, *b0, *cb, *phi, *acc, *nb, *gwb, *v, *r, *gdic;
-  int* sync;
+  int* sync;       // work, err, then done_fwd/bary_ready/done_bwd/msg_ready [4P]
+  SkProblem* prob; // device copy of the problem descriptor
   template <class A>
   void layout(A& al, size_t P, size_t K, size_t L, size_t N, bool b_init, bool fwd_only) {
     const size_t KN = K * N, PKN = P * KN, PN = P * N, slots = fwd_only ? 2 : L;
@@ -753,7 +754,8 @@ struct FusedBufs {
     f(v, fwd_only ? 1 : PKN);
     f(r, fwd_only ? 1 : PKN);
     f(gdic, fwd_only ? 1 : PKN);
-    alloc_into(al, reinterpret_cast<void**>(&sync), sk_sync_ints((int)P) * sizeof(int));
+    alloc_into(al, reinterpret_cast<void**>(&sync), (2 + 4 * P) * sizeof(int));
+    alloc_into(al, reinterpret_cast<void**>(&prob), sizeof(SkProblem));
   }
 };
 
@@ -791,30 +793,46 @@ int prepare_fused(wdl_ctx* ctx, FusedBufs& B, int P, int K, const double* atoms,
   return WDL_OK;
 }
 
-SkArgs fused_args(const FusedBufs& B, int P, int K, int L, int loss_type, const double* obs,
-                  bool fwd_only) {
+// Fills the problem descriptor, copies it to the device and launches.
+int launch_single(wdl_ctx* ctx, const FusedBufs& B, int P, int K, int L, int loss_type,
+                  const double* obs, bool fwd_only, bool need_dic, cudaStream_t s) {
+  SkProblem pr{};
+  sk_fill_geometry(pr, ctx->W, ctx->H, ctx->precision == WDL_SPLIT_BF16);
+  pr.K = K;
+  pr.L = L;
+  pr.P = P;
+  pr.loss_type = loss_type;
+  pr.fwd_only = fwd_only ? 1 : 0;
+  pr.need_dic = need_dic ? 1 : 0;
+  pr.atoms = B.atoms;
+  pr.lam = B.lam;
+  pr.obs = obs;
+  pr.b0 = B.b0;
+  pr.cb = B.cb;
+  pr.phi = B.phi;
+  pr.acc = B.acc;
+  pr.nb = B.nb;
+  pr.gwb = B.gwb;
+  pr.v = B.v;
+  pr.r = B.r;
+  pr.gdic = B.gdic;
+  pr.dot = B.dot;
+  pr.loss = B.loss;
+  pr.sync = B.sync + 2;
+  // Pageable source: the copy is staged before the call returns.
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(B.prob, &pr, sizeof(pr), cudaMemcpyHostToDevice, s));
   SkArgs a{};
-  a.P = P;
-  a.K = K;
-  a.L = L;
-  a.loss_type = loss_type;
-  a.fwd_only = fwd_only ? 1 : 0;
-  a.atoms = B.atoms;
-  a.lam = B.lam;
-  a.obs = obs;
-  a.b0 = B.b0;
-  a.cb = B.cb;
-  a.phi = B.phi;
-  a.acc = B.acc;
-  a.nb = B.nb;
-  a.gwb = B.gwb;
-  a.v = B.v;
-  a.r = B.r;
-  a.gdic = B.gdic;
-  a.dot = B.dot;
-  a.loss = B.loss;
+  a.G = ctx->G32[ctx->W >= ctx->H ? 0 : 1];
+  a.Gn = ctx->W >= ctx->H ? ctx->W : ctx->H;
+  a.nprobs = 1;
+  a.probs = B.prob;
+  a.items = nullptr;
+  a.total = (long long)sk_problem_items(pr);
   a.sync = B.sync;
-  return a;
+  int rc;
+  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
+  ctx->fused_sync = B.sync;
+  return WDL_OK;
 }
 
 int gradient_both_fused(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
@@ -835,8 +853,7 @@ int gradient_both_fused(wdl_ctx* ctx, int P, int K, int L, int loss_type, const 
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.acc, 0, (size_t)L * PN * 4, s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.nb, 0, 2 * PN * 4, s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gwb, 0, 2 * PN * 4, s));
-  SkArgs a = fused_args(B, P, K, L, loss_type, observed, false);
-  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
+  if ((rc = launch_single(ctx, B, P, K, L, loss_type, observed, false, true, s))) return rc;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
   k_sum_over_p_f32<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
   WDL_LAUNCH_CHECK(ctx);
@@ -850,7 +867,6 @@ int gradient_both_fused(wdl_ctx* ctx, int P, int K, int L, int loss_type, const 
     k_b_last<<<launch_cfg(ctx, PKN), 256, 0, s>>>(acc_L, B.phi + (size_t)(L - 1) * PKN, b_last, K, N, PKN);
     WDL_LAUNCH_CHECK(ctx);
   }
-  ctx->fused_sync = B.sync;
   return WDL_OK;
 }
 
@@ -864,11 +880,9 @@ int barycenter_fused(wdl_ctx* ctx, int P, int K, int L, const double* atoms, con
   B.layout(ctx->arena, P, K, L, N, false, true);
   if ((rc = prepare_fused(ctx, B, P, K, atoms, weights, nullptr, true, s))) return rc;
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.acc, 0, 2 * PN * 4, s));
-  SkArgs a = fused_args(B, P, K, L, WDL_LOSS_QUADRATIC, nullptr, true);
-  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
+  if ((rc = launch_single(ctx, B, P, K, L, WDL_LOSS_QUADRATIC, nullptr, true, false, s))) return rc;
   k_exp_to_double<<<launch_cfg(ctx, PN), 256, 0, s>>>(B.acc + (size_t)((L - 1) & 1) * PN, bary_out, PN);
   WDL_LAUNCH_CHECK(ctx);
-  ctx->fused_sync = B.sync;
   return WDL_OK;
 }
 

@@ -339,6 +339,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + 3 * kTileBytes + 16);
   int* s_int = reinterpret_cast<int*>(base + 3 * kTileBytes + 32);          // [2][4]
   double* s_dbl = reinterpret_cast<double*>(base + 3 * kTileBytes + 64);    // [2][kWarps]
+  SkProblem* s_prob = reinterpret_cast<SkProblem*>(base + 3 * kTileBytes + 256);  // [2]
 
   load_factor<SPLIT>(g_tile, a.G, a.Gn, tid, blockDim.x);
   if (tid == 0) {
@@ -366,73 +367,97 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   c.half = ws >> 2;
   c.phase = 0;
 
-  Geo g;
-  g.W = a.W;
-  g.H = a.H;
-  g.Wp = a.Wp;
-  g.Hp = a.Hp;
-  g.cpr = (uint32_t)(a.Wp / (SPLIT ? 8 : 4));
-  g.cpr_magic = (uint32_t)((0x100000000ull + g.cpr - 1) / g.cpr);
-  g.vec = a.vec != 0;
-  const int K = a.K, L = a.L, P = a.P;
-  const size_t N = a.N, PN = (size_t)P * N, PKN = (size_t)P * K * N;
-  const long long PK = (long long)P * K;
   int* work = a.sync;
   int* err = a.sync + 1;
-  int* done_fwd = a.sync + 2;
-  int* bary_ready = done_fwd + P;
-  int* done_bwd = bary_ready + P;
-  int* msg_ready = done_bwd + P;
-  // Tape slot of iteration it (1..L): all L kept for the reverse pass; two
-  // slots suffice for a forward-only run.
-  auto slot = [&](int it) -> size_t { return a.fwd_only ? (size_t)((it - 1) & 1) : (size_t)(it - 1); };
-
+  SkProblem* const pr = &s_prob[st];
+  int cur_q = -1;
   Trace tr;
   while (true) {
     tr.start(a.trace, t);
     tr.type = 0;
-    if (t == 0) s_int[st * 4] = atomicAdd(work, 1);
-    bar_sync(st, kSt);
-    const long long item = s_int[st * 4];
-    if (item >= a.total) break;
-    int type, step;  // type 0 = FWD, 1 = DICT, 2 = WGT
-    long long pk;
-    if (item < (long long)L * PK) {
-      type = 0;
-      step = (int)(item / PK) + 1;
-      pk = item % PK;
-    } else {
-      const long long j = item - (long long)L * PK;
-      step = L - (int)(j / (2 * PK));
-      const long long rem = j % (2 * PK);
-      pk = rem >> 1;
-      type = 1 + (int)(rem & 1);
+    if (t == 0) {
+      const int item = atomicAdd(work, 1);
+      int q = 0, type = 0, step = 0, pkv = 0;
+      if (item < a.total) {
+        if (a.items) {
+          const int4 d = a.items[item];
+          q = d.x; type = d.y; step = d.z; pkv = d.w;
+        } else {  // one problem: forward items, then per reverse step its items
+          const SkProblem& p0 = a.probs[0];
+          const long long PK = (long long)p0.P * p0.K;
+          if (item < (long long)p0.L * PK) {
+            type = 0;
+            step = (int)(item / PK) + 1;
+            pkv = (int)(item % PK);
+          } else {
+            const long long per = p0.need_dic ? 2 * PK : PK;
+            const long long j = item - (long long)p0.L * PK;
+            step = p0.L - (int)(j / per);
+            const long long rem = j % per;
+            pkv = (int)(p0.need_dic ? rem >> 1 : rem);
+            type = p0.need_dic ? 1 + (int)(rem & 1) : 2;
+          }
+        }
+      }
+      s_int[st * 4] = item < a.total ? q : -1;
+      s_int[st * 4 + 1] = type;
+      s_int[st * 4 + 2] = step;
+      s_int[st * 4 + 3] = pkv;
     }
-    const int p = (int)(pk / K), k = (int)(pk % K);
+    bar_sync(st, kSt);
+    const int q = s_int[st * 4];
+    if (q < 0) break;
+    const int type = s_int[st * 4 + 1], step = s_int[st * 4 + 2];
+    const long long pk = s_int[st * 4 + 3];
+    if (q != cur_q) {  // this stream's problem descriptor, staged in SMEM
+      const int nw = (int)(sizeof(SkProblem) / 4);
+      if (t < nw) reinterpret_cast<uint32_t*>(pr)[t] = reinterpret_cast<const uint32_t*>(&a.probs[q])[t];
+      cur_q = q;
+    }
+    bar_sync(st, kSt);
     tr.type = type;
+    const int K = pr->K, L = pr->L, P = pr->P;
+    const size_t N = pr->N, PN = (size_t)P * N, PKN = (size_t)P * K * N;
+    const int p = (int)(pk / K), k = (int)(pk % K);
+    Geo g;
+    g.W = pr->W;
+    g.H = pr->H;
+    g.Wp = pr->Wp;
+    g.Hp = pr->Hp;
+    g.cpr = pr->cpr;
+    g.cpr_magic = pr->cpr_magic;
+    g.vec = pr->vec != 0;
+    const bool fwd_only = pr->fwd_only != 0;
+    int* done_fwd = pr->sync;
+    int* bary_ready = done_fwd + P;
+    int* done_bwd = bary_ready + P;
+    int* msg_ready = done_bwd + P;
+    // Tape slot of iteration it (1..L): all L kept for the reverse pass; two
+    // slots suffice for a forward-only run.
+    auto slot = [&](int it) -> size_t { return fwd_only ? (size_t)((it - 1) & 1) : (size_t)(it - 1); };
     {  // every array this item reads, requested into L2 up front
       const size_t pkN = (size_t)pk * N, pN = (size_t)p * N;
       if (type == 0) {
         if (step > 1) {
-          prefetch_l2(a.acc + slot(step - 1) * PN + pN, N, t);
-          prefetch_l2(a.phi + slot(step - 1) * PKN + pkN, N, t);
-        } else if (a.b0) {
-          prefetch_l2(a.b0 + pkN, N, t);
+          prefetch_l2(pr->acc + slot(step - 1) * PN + pN, N, t);
+          prefetch_l2(pr->phi + slot(step - 1) * PKN + pkN, N, t);
+        } else if (pr->b0) {
+          prefetch_l2(pr->b0 + pkN, N, t);
         }
       } else {
         const int s = step;
-        prefetch_l2(a.phi + slot(s) * PKN + pkN, N, t);
-        prefetch_l2(a.cb + slot(s) * PKN + pkN, N, t);
-        if (s > 1) prefetch_l2(a.phi + slot(s - 1) * PKN + pkN, N, t);
+        prefetch_l2(pr->phi + slot(s) * PKN + pkN, N, t);
+        prefetch_l2(pr->cb + slot(s) * PKN + pkN, N, t);
+        if (s > 1) prefetch_l2(pr->phi + slot(s - 1) * PKN + pkN, N, t);
         if (type == 1) {
-          prefetch_l2(a.nb + (size_t)(s & 1) * PN + pN, N, t);
-          prefetch_l2(a.v + pkN, N, t);
-          prefetch_l2(a.acc + slot(s) * PN + pN, N, t);
-          prefetch_l2(a.gdic + pkN, N, t);
+          prefetch_l2(pr->nb + (size_t)(s & 1) * PN + pN, N, t);
+          prefetch_l2(pr->v + pkN, N, t);
+          prefetch_l2(pr->acc + slot(s) * PN + pN, N, t);
+          prefetch_l2(pr->gdic + pkN, N, t);
         } else {
-          prefetch_l2(a.gwb + (size_t)(s & 1) * PN + pN, N, t);
-          prefetch_l2(a.r + pkN, N, t);
-          if (s > 1) prefetch_l2(a.acc + slot(s - 1) * PN + pN, N, t);
+          prefetch_l2(pr->gwb + (size_t)(s & 1) * PN + pN, N, t);
+          prefetch_l2(pr->r + pkN, N, t);
+          if (s > 1) prefetch_l2(pr->acc + slot(s - 1) * PN + pN, N, t);
         }
       }
     }
@@ -452,32 +477,32 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       break;
     }
     tr.mark(1);
-    const float lam = a.lam[pk];
-    const float* atom = a.atoms + (size_t)k * N;
+    const float lam = pr->lam[pk];
+    const float* atom = pr->atoms + (size_t)k * N;
     bool ok = true;
 
     if (type == 0) {  // ---------------- forward Bregman iteration
       const int it = step;
-      float* cb_out = a.cb + slot(it) * PKN + pk * N;
-      float* phi_out = a.phi + slot(it) * PKN + pk * N;
-      float* acc_out = a.acc + slot(it) * PN + (size_t)p * N;
+      float* cb_out = pr->cb + slot(it) * PKN + pk * N;
+      float* phi_out = pr->phi + slot(it) * PKN + pk * N;
+      float* acc_out = pr->acc + slot(it) * PN + (size_t)p * N;
       if (it == 1) {
-        if (a.b0) {
-          const float* src[1] = {a.b0 + pk * N};
+        if (pr->b0) {
+          const float* src[1] = {pr->b0 + pk * N};
           stage_rows<SPLIT, 1>(c.tile, src, [](const float (&v)[1]) { return v[0]; }, g, t);
         } else {
           const float* src[1] = {atom};
           stage_rows<SPLIT, 0>(c.tile, src, [](const float (&)[1]) { return 1.f; }, g, t);
         }
       } else {  // b[it-1] = exp(acc[it-1]) / phi[it-1]
-        const float* src[2] = {a.acc + slot(it - 1) * PN + (size_t)p * N,
-                               a.phi + slot(it - 1) * PKN + pk * N};
+        const float* src[2] = {pr->acc + slot(it - 1) * PN + (size_t)p * N,
+                               pr->phi + slot(it - 1) * PKN + pk * N};
         stage_rows<SPLIT, 2>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
       }
       tr.mark(2);
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
       tr.mark(3);
-      const bool keep_cb = !a.fwd_only;
+      const bool keep_cb = !fwd_only;
       const float* msrc[1] = {atom};
       mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
         if (keep_cb) __stcg(cb_out + idx, y);
@@ -495,30 +520,30 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       tr.mark(6);
     } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
       const int s = step;
-      const float* src[4] = {a.nb + (size_t)(s & 1) * PN + (size_t)p * N, a.v + pk * N,
-                             a.acc + slot(s) * PN + (size_t)p * N, a.phi + slot(s) * PKN + pk * N};
+      const float* src[4] = {pr->nb + (size_t)(s & 1) * PN + (size_t)p * N, pr->v + pk * N,
+                             pr->acc + slot(s) * PN + (size_t)p * N, pr->phi + slot(s) * PKN + pk * N};
       stage_rows<SPLIT, 4>(c.tile, src,
                            [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); },
                            g, t);
       tr.mark(2);
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
       tr.mark(3);
-      const float* cbp = a.cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
-      float* gd = a.gdic + pk * N;
+      const float* cbp = pr->cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
+      float* gd = pr->gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
       mid_columns<SPLIT, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
         const float rc = frcp(in[0]);
-        const float q = y * rc;
-        __stcg(gd + idx, in[1] + q);
-        return -in[2] * q * rc;
+        const float q2 = y * rc;
+        __stcg(gd + idx, in[1] + q2);
+        return -in[2] * q2 * rc;
       }, s > 1);
       tr.mark(4);
       if (s > 1) {
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
         tr.mark(5);
-        const float* php = a.phi + slot(s - 1) * PKN + pk * N;
-        float* vout = a.v + pk * N;
-        float* nout = a.nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
+        const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
+        float* vout = pr->v + pk * N;
+        float* nout = pr->nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[1] = {php};
         epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
           const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
@@ -530,20 +555,20 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       }
     } else {  // ---------------- reverse pass, weight recursion
       const int s = step;
-      const float* src[3] = {a.gwb + (size_t)(s & 1) * PN + (size_t)p * N, a.r + pk * N,
-                             a.phi + slot(s) * PKN + pk * N};
+      const float* src[3] = {pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N, pr->r + pk * N,
+                             pr->phi + slot(s) * PKN + pk * N};
       double dacc = 0;
       stage_rows<SPLIT, 3>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
         dacc += (double)__logf(v[2]) * (double)v[0];
         return fdiv(lam * v[0] - v[1], v[2]);
       }, g, t);
       const double dsum = st_sum(dacc, s_dbl, st, t);
-      if (t == 0) atomicAdd(&a.dot[pk], dsum);
+      if (t == 0) atomicAdd(&pr->dot[pk], dsum);
       tr.mark(2);
       if (s > 1) {
         ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
         tr.mark(3);
-        const float* cbp = a.cb + slot(s) * PKN + pk * N;
+        const float* cbp = pr->cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
         mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
@@ -552,10 +577,10 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         tr.mark(4);
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
         tr.mark(5);
-        const float* php = a.phi + slot(s - 1) * PKN + pk * N;
-        const float* accp = a.acc + slot(s - 1) * PN + (size_t)p * N;
-        float* rout = a.r + pk * N;
-        float* gout = a.gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
+        const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
+        const float* accp = pr->acc + slot(s - 1) * PN + (size_t)p * N;
+        float* rout = pr->r + pk * N;
+        float* gout = pr->gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[2] = {accp, php};
         epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
           const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
@@ -579,7 +604,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       __threadfence();
       int fin;
       if (type == 0) fin = atomicAdd(&done_fwd[p], 1) + 1 == step * K;
-      else fin = atomicAdd(&done_bwd[p], 1) + 1 == 2 * K * (L - step + 1);
+      else fin = atomicAdd(&done_bwd[p], 1) + 1 == (pr->need_dic ? 2 : 1) * K * (L - step + 1);
       s_int[st * 4 + 2] = fin;
     }
     bar_sync(st, kSt);
@@ -591,41 +616,43 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     __threadfence();
     if (type == 0) {
       const int it = step;
-      if (a.fwd_only && it >= 2) {
+      if (fwd_only && it >= 2) {
         // acc[it-1] has been read by every item of iteration it: clear its slot,
         // which iteration it+1 accumulates into.
-        float* z = a.acc + slot(it + 1) * PN + (size_t)p * N;
+        float* z = pr->acc + slot(it + 1) * PN + (size_t)p * N;
         for (size_t j = t; j < N; j += kSt) __stcg(z + j, 0.f);
       }
-      const bool last = it == L && !a.fwd_only;
+      const bool last = it == L && !fwd_only;
       if (last) {  // loss and its gradient (cpp/loss.h:19-90); messages for s = L
-        const float* accL = a.acc + slot(L) * PN + (size_t)p * N;
-        float* n0 = a.nb + (size_t)(L & 1) * PN + (size_t)p * N;
-        float* g0 = a.gwb + (size_t)(L & 1) * PN + (size_t)p * N;
+        const float* accL = pr->acc + slot(L) * PN + (size_t)p * N;
+        float* n0 = pr->nb + (size_t)(L & 1) * PN + (size_t)p * N;
+        float* g0 = pr->gwb + (size_t)(L & 1) * PN + (size_t)p * N;
+        const bool dic = pr->need_dic != 0;
+        const int lt = pr->loss_type;
         double lacc = 0;
         for (size_t j = t; j < N; j += kSt) {
           const float bv = expf(__ldcg(accL + j));
-          const double o = a.obs[(size_t)p * N + j];
+          const double o = pr->obs[(size_t)p * N + j];
           const float o32 = (float)o;
           float gg;
-          if (a.loss_type == WDL_LOSS_TV) {
+          if (lt == WDL_LOSS_TV) {
             lacc += fabs((double)bv - o);
             gg = (bv - o32) > 0.f ? 0.5f : -0.5f;
-          } else if (a.loss_type == WDL_LOSS_QUADRATIC) {
+          } else if (lt == WDL_LOSS_QUADRATIC) {
             const double d = (double)bv - o;
             lacc += d * d;
             gg = 2.f * (bv - o32);
           } else {
             const double rr = (double)bv / o;
             lacc += (double)bv * log(rr > kEpsilon ? rr : kEpsilon) - (double)bv + o;
-            const float q = bv / o32;
-            gg = q > 0.f ? logf(q) : (float)kLogEpsilon;
+            const float q2 = bv / o32;
+            gg = q2 > 0.f ? logf(q2) : (float)kLogEpsilon;
           }
-          __stcg(n0 + j, gg);
+          if (dic) __stcg(n0 + j, gg);
           __stcg(g0 + j, gg * bv);
         }
         const double tot = st_sum(lacc, s_dbl, st, t);
-        if (t == 0) a.loss[p] = a.loss_type == WDL_LOSS_TV ? 0.5 * tot : tot;
+        if (t == 0) pr->loss[p] = lt == WDL_LOSS_TV ? 0.5 * tot : tot;
       }
       bar_sync(st, kSt);
       if (t == 0) {
@@ -636,10 +663,11 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     } else {
       const int s = step;
       if (s > 1) {  // the messages step s consumed are cleared for step s-2's sums
-        float* zn = a.nb + (size_t)(s & 1) * PN + (size_t)p * N;
-        float* zg = a.gwb + (size_t)(s & 1) * PN + (size_t)p * N;
+        float* zn = pr->nb + (size_t)(s & 1) * PN + (size_t)p * N;
+        float* zg = pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N;
+        const bool dic = pr->need_dic != 0;
         for (size_t j = t; j < N; j += kSt) {
-          __stcg(zn + j, 0.f);
+          if (dic) __stcg(zn + j, 0.f);
           __stcg(zg + j, 0.f);
         }
       }
@@ -657,46 +685,53 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   if (warp == 0) ptx::tmem_dealloc(*tmem_slot, 2 * kTmemCols);
 }
 
-__global__ void k_sync_init(int* sync, int P) {
-  for (int i = threadIdx.x; i < 2 + 4 * P; i += blockDim.x) {
-    int v = 0;
-    if (i >= 2 + 3 * P) v = -1;  // msg_ready
-    sync[i] = v;
+// Per-problem sync words: done_fwd, bary_ready (0), done_bwd, msg_ready (-1).
+__global__ void k_sync_init(int* work_err, const SkProblem* probs, int nprobs) {
+  if (blockIdx.x == 0 && threadIdx.x < 2) work_err[threadIdx.x] = 0;
+  for (int q = blockIdx.x; q < nprobs; q += gridDim.x) {
+    const int P = probs[q].P;
+    int* s = probs[q].sync;
+    for (int i = threadIdx.x; i < 4 * P; i += blockDim.x) s[i] = i >= 3 * P ? -1 : 0;
   }
 }
 
 }  // namespace
 
-size_t sk_sync_ints(int P) { return 2 + 4 * (size_t)P; }
+void sk_fill_geometry(SkProblem& pr, int W, int H, bool split_bf16) {
+  pr.W = W;
+  pr.H = H;
+  pr.Wp = (W + 15) & ~15;
+  pr.Hp = (H + 15) & ~15;
+  pr.N = (size_t)W * H;
+  pr.vec = (W % 4) == 0;
+  pr.cpr = (uint32_t)(pr.Wp / (split_bf16 ? 8 : 4));  // 16-byte operand chunks per row
+  pr.cpr_magic = (uint32_t)((0x100000000ull + pr.cpr - 1) / pr.cpr);
+}
+
+size_t sk_problem_items(const SkProblem& pr) {
+  const size_t PK = (size_t)pr.P * pr.K;
+  if (pr.fwd_only) return (size_t)pr.L * PK;
+  return (size_t)pr.L * PK * (1 + (pr.need_dic ? 2 : 1));
+}
 
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
-  a.W = ctx->W;
-  a.H = ctx->H;
-  a.Wp = (a.W + 15) & ~15;
-  a.Hp = (a.H + 15) & ~15;
-  a.Gn = a.W >= a.H ? a.W : a.H;
-  a.G = ctx->G32[a.W >= a.H ? 0 : 1];
-  a.N = ctx->N;
-  a.vec = (a.W % 4) == 0;
-  const long long PK = (long long)a.P * a.K;
-  a.total = a.fwd_only ? (long long)a.L * PK : 3LL * a.L * PK;
-  k_sync_init<<<1, 256, 0, s>>>(a.sync, a.P);
-  WDL_LAUNCH_CHECK(ctx);
-  const size_t smem = 3 * tc::kTileBytes + 1024 + 256;
+  const size_t smem = 3 * tc::kTileBytes + 1024 + 256 + 2 * sizeof(SkProblem) + 64;
   const bool split = ctx->precision == WDL_SPLIT_BF16;
+  k_sync_init<<<a.nprobs < 256 ? a.nprobs : 256, 128, 0, s>>>(a.sync, a.probs, a.nprobs);
+  WDL_LAUNCH_CHECK(ctx);
   if (split)
     WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   else
     WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long streams = (a.total + 1) / 2;
   const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
-  if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
   a.trace = nullptr;
   if (ctx->trace_level >= 2) {
     if (!ctx->d_trace) WDL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_trace, 27 * sizeof(unsigned long long)));
     WDL_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_trace, 0, 27 * sizeof(unsigned long long), s));
     a.trace = ctx->d_trace;
   }
+  if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
   if (split) sinkhorn_tc_kernel<true><<<grid, 2 * kSt, smem, s>>>(a);
   else sinkhorn_tc_kernel<false><<<grid, 2 * kSt, smem, s>>>(a);
   WDL_LAUNCH_CHECK(ctx);
@@ -707,10 +742,7 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
     cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b);
     ctx->conv_ms += ms;
     ctx->conv_launches += 1;
-    // operator applications: 2 per FWD item, 2 per reverse item with s > 1,
-    // 1 per dictionary item at s = 1
-    const double convs = a.fwd_only ? 2.0 * a.L * PK : 2.0 * a.L * PK + 4.0 * (a.L - 1) * PK + PK;
-    ctx->conv_images += convs;
+    ctx->conv_images += (double)a.total;  // work items (two operator applications each, at most)
   }
   return WDL_OK;
 }

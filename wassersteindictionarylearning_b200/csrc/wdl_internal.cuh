@@ -173,10 +173,15 @@ int tc_check_status(wdl_ctx* ctx);
 bool tc_supported(const wdl_ctx* ctx);
 
 // Fused persistent tensor-core Sinkhorn kernel (sinkhorn_tc.cu).
-struct SkArgs {
-  int P, K, L, W, H, Wp, Hp, Gn, loss_type, fwd_only, vec;
+// One problem of a fused launch: P histograms on one W x H grid (sides <= 128)
+// against K atoms, L iterations.  Pointers are device buffers of this problem.
+struct SkProblem {
+  int W, H, Wp, Hp, K, L, P, loss_type;
+  int fwd_only;   // forward only (barycenters): two tape slots, no loss
+  int need_dic;   // run the dictionary recursion (atom gradient); 0 = weights only
+  int vec;        // rows are 16-byte aligned (W % 4 == 0)
+  uint32_t cpr, cpr_magic;  // operand chunks per row, ceil(2^32 / cpr)
   size_t N;
-  const float* G;
   const float* atoms;    // [K][N]
   const float* lam;      // [P][K]
   const double* obs;     // [P][N]
@@ -188,11 +193,21 @@ struct SkArgs {
   float *v, *r, *gdic;   // [P][K][N]
   double* dot;           // [P][K]
   double* loss;          // [P]
-  int* sync;             // work, err, done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P]
-  unsigned long long* trace;  // [3 item types][8 phases + 1 count] ns, or null
-  long long total;
+  int* sync;             // done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P]
 };
-size_t sk_sync_ints(int P);
+
+struct SkArgs {
+  const float* G;        // factor matrix of the launch's gamma, Gn x Gn
+  int Gn, nprobs;
+  const SkProblem* probs;     // device array [nprobs]
+  const int4* items;          // (problem, type, step, pk) per work item, or null: problem 0
+  long long total;            // work items
+  int* sync;                  // work counter, error word
+  unsigned long long* trace;  // [3 item types][8 phases + 1 count] ns, or null
+};
+// Host helpers of the fused launch.
+void sk_fill_geometry(SkProblem& pr, int W, int H, bool split_bf16);
+size_t sk_problem_items(const SkProblem& pr);
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s);
 int sinkhorn_tc_status(wdl_ctx* ctx, int* sync_dev);
 
