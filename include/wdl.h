@@ -194,7 +194,9 @@ int wdl_convolve_device_noalloc(wdl_ctx* ctx, const double* u, double* out, int 
  * library counts one), and the time in the dominant kernel (the separable
  * operator, or the fused Sinkhorn kernel on the tensor-core path) measured with
  * CUDA events on the launching stream since profiling was switched on
- * (level >= 1; the events synchronise each launch).  Level 2 also records a
+ * (level >= 1; the events synchronise each launch); conv_images counts the
+ * separable-operator applications those launches performed (an image through
+ * both axes is one).  Level 2 also records a
  * device-side phase trace of the fused kernel: wdl_phase_trace returns 27
  * values, for item types forward / dictionary / weights, 8 accumulated phase
  * times in ns (claim, dependency wait, prologue, first operator, mid step,

@@ -304,6 +304,7 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
   a.probs = reinterpret_cast<SkProblem*>(base + sz.probs);
   a.items = reinterpret_cast<int4*>(base + items_off);
   a.total = (long long)n_items;
+  for (int q = 0; q < nprob; ++q) a.apps += sk_problem_applications(prs[q]);
   a.sync = reinterpret_cast<int*>(base + sz.gsync);
   if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
   ctx->fused_sync = a.sync;

@@ -828,6 +828,7 @@ int launch_single(wdl_ctx* ctx, const FusedBufs& B, int P, int K, int L, int los
   a.probs = B.prob;
   a.items = nullptr;
   a.total = (long long)sk_problem_items(pr);
+  a.apps = sk_problem_applications(pr);
   a.sync = B.sync;
   int rc;
   if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;

@@ -714,6 +714,15 @@ size_t sk_problem_items(const SkProblem& pr) {
   return (size_t)pr.L * PK * (1 + (pr.need_dic ? 2 : 1));
 }
 
+// Separable-operator applications of one problem's items: 2 per forward item,
+// 2 per dictionary item (1 at step 1), 2 per weight item (none at step 1) —
+// (6L-4) per atom and histogram with the dictionary recursion, (4L-2) without.
+double sk_problem_applications(const SkProblem& pr) {
+  const double PK = (double)pr.P * pr.K, L = pr.L;
+  if (pr.fwd_only) return 2 * L * PK;
+  return PK * (2 * L + (pr.need_dic ? 2 * L - 1 : 0) + 2 * (L - 1));
+}
+
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
   const size_t smem = 3 * tc::kTileBytes + 1024 + 256 + 2 * sizeof(SkProblem) + 64;
   const bool split = ctx->precision == WDL_SPLIT_BF16;
@@ -742,7 +751,7 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
     cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b);
     ctx->conv_ms += ms;
     ctx->conv_launches += 1;
-    ctx->conv_images += (double)a.total;  // work items (two operator applications each, at most)
+    ctx->conv_images += a.apps;
   }
   return WDL_OK;
 }

@@ -202,12 +202,14 @@ struct SkArgs {
   const SkProblem* probs;     // device array [nprobs]
   const int4* items;          // (problem, type, step, pk) per work item, or null: problem 0
   long long total;            // work items
+  double apps;                // operator applications the items perform (for profiling)
   int* sync;                  // work counter, error word
   unsigned long long* trace;  // [3 item types][8 phases + 1 count] ns, or null
 };
 // Host helpers of the fused launch.
 void sk_fill_geometry(SkProblem& pr, int W, int H, bool split_bf16);
 size_t sk_problem_items(const SkProblem& pr);
+double sk_problem_applications(const SkProblem& pr);
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s);
 int sinkhorn_tc_status(wdl_ctx* ctx, int* sync_dev);
 
