@@ -96,70 +96,118 @@ int axis_pass(wdl_ctx* ctx, const T* in, T* out, const T* G, int R, int C, size_
 // two passes per output: the maximum of the exponents, then the shifted sum
 // (cpp/kernels.h:1082-1091).  With signs, s_k = +-1 from in_sign and the sign of
 // the sum goes to out_sign, log|sum| to out (cpp/kernels.h:1123-1136).
-// A block owns LR rows of one image and produces every output of those rows.
+//
+// A block owns LR rows of one image (staged in SMEM with an odd row stride, so
+// the 16 rows a warp reads at one tap fall in 16 different banks) and produces
+// every output of those rows.  Taps are visited outwards from k = c.  With
+// X = max_k in[r][k], every tap at distance >= d has exponent <= -d^2/gamma + X,
+// so:
+//  * the maximum pass stops at the first d where -d^2/gamma + X <= max so far;
+//  * the sum pass stops at the first d where -d^2/gamma + X < max - kTail; the
+//    taps left out then add at most 2C e^-kTail relative to the largest term,
+//    below the rounding of the sum (kTail = 40 bits for FP32, 60 nats for FP64),
+//    so the result is the full sum's to rounding.
+// FP32 works in base 2 (inputs scaled by log2 e once when staged; ex2 / lg2),
+// FP64 in base e with exp / log.  The summation order (outwards, both sides)
+// differs from the reference's k = 0..C-1; only rounding depends on it.
 constexpr int LR = 16;
 
 template <typename T>
-__device__ __forceinline__ T dev_exp(T x);
+struct LogOps;
 template <>
-__device__ __forceinline__ float dev_exp<float>(float x) { return expf(x); }
+struct LogOps<float> {
+  static constexpr float kScale = 1.4426950408889634f;   // log2 e: natural -> base 2
+  static constexpr float kUnscale = 0.6931471805599453f;  // ln 2
+  static constexpr float kTail = 40.f;                   // bits
+  static constexpr float kFloor = -3.402823466e38f;      // start of the maximum
+  __device__ static float ex(float x) { return exp2f(x); }
+  __device__ static float lg(float x) { return log2f(x); }
+};
 template <>
-__device__ __forceinline__ double dev_exp<double>(double x) { return exp(x); }
-template <typename T>
-__device__ __forceinline__ T dev_log(T x);
-template <>
-__device__ __forceinline__ float dev_log<float>(float x) { return logf(x); }
-template <>
-__device__ __forceinline__ double dev_log<double>(double x) { return log(x); }
+struct LogOps<double> {
+  static constexpr double kScale = 1.0;
+  static constexpr double kUnscale = 1.0;
+  static constexpr double kTail = 60.0;   // nats
+  static constexpr double kFloor = -1e99;  // the reference's start (cpp/kernels.h:1083)
+  __device__ static double ex(double x) { return exp(x); }
+  __device__ static double lg(double x) { return log(x); }
+};
 
 template <typename T, bool SIGNED>
 __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign) {
+  using Op = LogOps<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* rows = reinterpret_cast<T*>(smem_raw);           // [LR][C]
-  T* lk = rows + LR * C;                                // [C] : -d^2/gamma
-  uint8_t* sg = reinterpret_cast<uint8_t*>(lk + C);     // [LR][C]
+  const int CP = C + 1;                                 // odd row stride (elements)
+  T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
+  T* lk = rows + LR * CP;                               // [C]: -d^2/gamma (scaled)
+  T* xmax = lk + C;                                     // [LR]
+  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);  // [LR][C + 4] (bank-spread bytes)
+  const int SP = C + 4;
   const int r0 = blockIdx.x * LR;
   const size_t base = (size_t)blockIdx.y * img_stride;
   const int nr = min(LR, R - r0);
-  for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
-    int rr = e / C, k = e - rr * C;
-    T v = T(0);
-    uint8_t sv = 1;
-    if (rr < nr) {
-      v = in[base + (size_t)(r0 + rr) * C + k];
-      if (SIGNED) sv = in_sign[base + (size_t)(r0 + rr) * C + k];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // stage: warp w owns rows w and w + 8, so the row maxima come from shuffles
+  for (int rr = warp; rr < LR; rr += 8) {
+    T vm = Op::kFloor;
+    for (int k = lane; k < C; k += 32) {
+      T v = Op::kFloor;
+      uint8_t sv = 1;
+      if (rr < nr) {
+        v = in[base + (size_t)(r0 + rr) * C + k] * Op::kScale;
+        if (SIGNED) sv = in_sign[base + (size_t)(r0 + rr) * C + k];
+      }
+      rows[rr * CP + k] = v;
+      if (SIGNED) sg[rr * SP + k] = sv;
+      vm = v > vm ? v : vm;
     }
-    rows[e] = v;
-    if (SIGNED) sg[e] = sv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const T w = __shfl_xor_sync(0xffffffffu, vm, o);
+      vm = w > vm ? w : vm;
+    }
+    if (lane == 0) xmax[rr] = vm;
   }
-  for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d * d) / gamma_t;
+  for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d) * T(d) / gamma_t * Op::kScale;
   __syncthreads();
   // Thread -> (c, rr) with rr fastest so that stores out[c][r0+rr] are contiguous.
   for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
-    int c = e / LR, rr = e - c * LR;
+    const int c = e / LR, rr = e - c * LR;
     if (rr >= nr) continue;
-    const T* row = rows + rr * C;
-    // The reference starts the maximum at -1e99 (FP64); FP32 uses -FLT_MAX so that
-    // an all -inf row still sums to 0 and returns -inf instead of NaN.
-    T vmax = sizeof(T) == 8 ? T(-1e99) : T(-3.402823466e38);
-    for (int k = 0; k < C; ++k) {
-      T t = lk[abs(c - k)] + row[k];
-      vmax = t > vmax ? t : vmax;
+    const T* row = rows + rr * CP;
+    const T X = xmax[rr];
+    T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
+    for (int d = 1; d < C; ++d) {
+      const T l = lk[d];
+      if (l + X <= m) break;
+      if (c - d >= 0) { const T t = l + row[c - d]; m = t > m ? t : m; }
+      if (c + d < C) { const T t = l + row[c + d]; m = t > m ? t : m; }
     }
-    T sum = T(0);
-    for (int k = 0; k < C; ++k) {
-      T ex = dev_exp<T>(lk[abs(c - k)] + row[k] - vmax);
-      if (SIGNED) sum += sg[rr * C + k] ? ex : -ex;
-      else sum += ex;
+    const uint8_t* sgn = sg + rr * SP;
+    T sum = Op::ex(row[c] - m);
+    if (SIGNED && !sgn[c]) sum = -sum;
+    const T floor_ = m - Op::kTail;
+    for (int d = 1; d < C; ++d) {
+      const T l = lk[d];
+      if (l + X < floor_) break;
+      const T lm = l - m;
+      if (c - d >= 0) {
+        const T ex = Op::ex(lm + row[c - d]);
+        sum += (!SIGNED || sgn[c - d]) ? ex : -ex;
+      }
+      if (c + d < C) {
+        const T ex = Op::ex(lm + row[c + d]);
+        sum += (!SIGNED || sgn[c + d]) ? ex : -ex;
+      }
     }
-    size_t o = base + (size_t)c * R + (r0 + rr);
+    const size_t o = base + (size_t)c * R + (r0 + rr);
     if (SIGNED) {
       out_sign[o] = sum >= T(0) ? 1 : 0;
-      out[o] = dev_log<T>(fabs(sum)) + vmax;
+      out[o] = (Op::lg(fabs(sum)) + m) * Op::kUnscale;
     } else {
-      out[o] = dev_log<T>(sum) + vmax;
+      out[o] = (Op::lg(sum) + m) * Op::kUnscale;
     }
   }
 }
@@ -167,7 +215,7 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
 template <typename T>
 int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
                   const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
-  size_t smem = (size_t)LR * C * sizeof(T) + C * sizeof(T) + (size_t)LR * C + 16;
+  size_t smem = ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
   const T gamma_t = T(ctx->gamma);
   size_t done = 0;
   while (done < nimg) {
