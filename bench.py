@@ -14,6 +14,11 @@ across ranks with one NCCL all-reduce per step (the path's only exchange).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision split_bf16|tf32|fp32|fp64]
     python bench.py --impl reference      # the reference's own CPU path (oracle/_ref)
+
+The headline line is the batched 128x128 workload.  `--workload dict64`
+(64x64, K=4, L=25, gamma=2, quadratic, FP32 kernel domain) and `--workload
+log256` (256x256, K=8, L=200, gamma=0.5, TV, FP32 log domain) measure the
+other two dictionary-learning configurations the same way.
 """
 from __future__ import annotations
 
@@ -32,9 +37,28 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd Sinkhorn iters/s (128², K=5) vs plain FP32; p50/p99 serve latency"
 UNIT = "hist-iter/s"
-WORKLOAD = dict(name="batched128", P=64, W=128, H=128, K=5, L=100, gamma=1.0, loss=4,
-                n_blobs=(2, 5))
-CPU_SAMPLE_P = 4  # histograms in the bounded CPU sample (full L)
+WORKLOADS = {
+    "batched128": dict(name="batched128", P=64, W=128, H=128, K=5, L=100, gamma=1.0, loss=4,
+                       loss_name="KL", n_blobs=(2, 5), std_frac=(0.03, 0.12), domain="kernel",
+                       precision=None, cpu_P=4, cpu_L=100),
+    "dict64": dict(name="dict64", P=16, W=64, H=64, K=4, L=25, gamma=2.0, loss=2,
+                   loss_name="quadratic", n_blobs=(1, 3), std_frac=(0.03, 0.12), domain="kernel",
+                   precision="fp32", cpu_P=16, cpu_L=25),
+    "log256": dict(name="log256", P=32, W=256, H=256, K=8, L=200, gamma=0.5, loss=1,
+                   loss_name="TV", n_blobs=(1, 3), std_frac=(0.01, 0.04), domain="log",
+                   precision="fp32", cpu_P=1, cpu_L=4),
+}
+
+
+def metric_for(wl):
+    if wl["name"] == "batched128":
+        return METRIC
+    return f"fwd+bwd Sinkhorn iters/s ({wl['W']}x{wl['H']}, K={wl['K']}, {wl['domain']} domain)"
+
+
+def describe(wl):
+    return (f"{wl['name']}: P={wl['P']} per GPU, {wl['W']}x{wl['H']}, K={wl['K']}, L={wl['L']}, "
+            f"gamma={wl['gamma']:g}, {wl['loss_name']} loss, {wl['domain']} domain")
 
 
 def parse():
@@ -43,6 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched128", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -78,32 +103,37 @@ def cpu_model():
     return "unknown"
 
 
-def time_cpu_reference(steps=1, warmup=0):
-    """The reference's own evaluate_both (GaussianSSE2DKernel, OpenMP over all
-    host cores) on a bounded sample: CPU_SAMPLE_P histograms at the full L."""
+def time_cpu_reference(wl, steps=1, warmup=0):
+    """The reference's own evaluate_both (GaussianSSE2DKernel, or the
+    LogSignArray kernel in the log domain, OpenMP over all host cores) on a
+    bounded sample: wl['cpu_P'] histograms at wl['cpu_L'] iterations."""
     from oracle import oracle as orc
     from wassersteindictionarylearning_b200.synthetic import make_problem, to_variables
-    w = WORKLOAD
-    P = CPU_SAMPLE_P
-    cfg, obs, atoms, wts = make_problem(None, seed=0, P=P, W=w["W"], H=w["H"], K=w["K"], L=w["L"],
-                                        gamma=w["gamma"], loss=w["loss"], n_blobs=w["n_blobs"])
+    w = wl
+    P, L = w["cpu_P"], w["cpu_L"]
+    log_domain = w["domain"] == "log"
+    cfg, obs, atoms, wts = make_problem(None, seed=0, P=P, W=w["W"], H=w["H"], K=w["K"], L=L,
+                                        gamma=w["gamma"], loss=w["loss"], n_blobs=w["n_blobs"],
+                                        std_frac=w["std_frac"])
     x = to_variables(wts, atoms, cfg["scale_dic"])
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
     if orc.ref_available():
         lib, kind = orc.RefLib(), "reference"
 
         def run():
-            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], w["L"], w["loss"],
-                                     cfg["scale_dic"], x, obs, kind=1)
+            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], L, w["loss"],
+                                     cfg["scale_dic"], x, obs, log_domain=log_domain, kind=1)
         cores = lib.omp_threads()
-        what = "GaussianSSE2DKernel evaluate_both (cpp/inverseWasserstein.h:986), OpenMP"
+        what = ("LogSignArrayGaussian2DKernel" if log_domain else "GaussianSSE2DKernel") + \
+            " evaluate_both (cpp/inverseWasserstein.h:986), OpenMP"
     else:
         lib, kind = orc.OracleLib(), "port"
         cores = cpu_threads()
 
         def run():
-            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], w["L"], w["loss"],
-                                     cfg["scale_dic"], x, obs, nthreads=cores)
+            return lib.evaluate_both(w["W"], w["H"], 1, w["gamma"], P, w["K"], L, w["loss"],
+                                     cfg["scale_dic"], x, obs, log_domain=log_domain,
+                                     nthreads=cores)
         what = "C restatement evaluate_both, OpenMP over histograms"
     for _ in range(warmup):
         run()
@@ -113,22 +143,25 @@ def time_cpu_reference(steps=1, warmup=0):
         run()
         times.append(time.perf_counter() - t0)
     per_step = statistics.median(times)
-    units = P * w["L"]
+    units = P * L
     return dict(value=units / per_step, unit=UNIT, cores=cores, kind=kind,
-                sample=f"{what}; {P} of 64 histograms at full size (128x128, K=5, L=100, KL), "
-                       f"{units} hist-iters per step, median of {steps}; CPU: {cpu_model()}"), per_step
+                sample=f"{what}; {P} of {w['P']} histograms, L={L} of {w['L']} ({w['W']}x{w['H']}, "
+                       f"K={w['K']}, {w['loss_name']}), {units} hist-iters per step, median of "
+                       f"{steps}; CPU: {cpu_model()}"), per_step
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    base, per_step = time_cpu_reference(steps=args.steps, warmup=min(args.warmup, 1))
-    line = dict(metric=METRIC, value=base["value"], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+    wl = WORKLOADS[args.workload]
+    base, per_step = time_cpu_reference(wl, steps=args.steps, warmup=min(args.warmup, 1))
+    line = dict(metric=metric_for(wl), value=base["value"], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
                 warmup=args.warmup, ms_per_step=per_step * 1e3, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                config=dict(workload=WORKLOAD["name"], P=CPU_SAMPLE_P, W=128, H=128, K=5, L=100,
-                            gamma=1.0, loss="KL", note="bounded sample of the batched workload"),
+                config=dict(workload=describe(wl), P=wl["cpu_P"], W=wl["W"], H=wl["H"], K=wl["K"],
+                            L=wl["cpu_L"], gamma=wl["gamma"], loss=wl["loss_name"],
+                            note="bounded sample of the workload"),
                 impl="reference", cpu_baseline=base,
                 e2e=dict(value=base["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
@@ -208,8 +241,8 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    precision = args.precision or default_precision()
-    wl = dict(WORKLOAD)
+    wl = dict(WORKLOADS[args.workload])
+    precision = args.precision or wl["precision"] or default_precision()
     if args.P:
         wl["P"] = args.P
     if args.L:
@@ -217,12 +250,16 @@ def run_ours(args):
     P, W, H, K, L = wl["P"], wl["W"], wl["H"], wl["K"], wl["L"]
     N = W * H
     cfg, obs, atoms, wts = make_problem(None, seed=1000 * rank, P=P, W=W, H=H, K=K, L=L,
-                                        gamma=wl["gamma"], loss=wl["loss"], n_blobs=wl["n_blobs"])
+                                        gamma=wl["gamma"], loss=wl["loss"], n_blobs=wl["n_blobs"],
+                                        std_frac=wl["std_frac"])
     sd = cfg["scale_dic"]
     x = to_variables(wts, atoms, sd)
     n = x.size
     PK = P * K
-    kern = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
+    if wl["domain"] == "log":
+        kern = w.CudaLogSignArrayGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
+    else:
+        kern = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
     ctx = kern.ctx
     L_ = _lib.lib()
     dev = torch.device("cuda", local)
@@ -282,6 +319,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     conv_ms, conv_launches, conv_imgs = C.c_double(), C.c_longlong(), C.c_double()
     L_.wdl_conv_profile(ctx, C.byref(conv_ms), C.byref(conv_launches), C.byref(conv_imgs))
+    exps = C.c_double()
+    L_.wdl_exp_profile(ctx, C.byref(exps))
     L_.wdl_set_profiling(ctx, 0)
     peaks = {}
     try:
@@ -295,7 +334,26 @@ def run_ours(args):
     # algorithmic (useful) FLOPs: one dense contraction per operator application;
     # the split-BF16 form executes three tensor products for each
     achieved_tflops = flop_per_img * imgs_per_launch / (conv_launch_ms * 1e-3) / 1e12
-    if precision in ("split_bf16", "tf32"):
+    if wl["domain"] == "log":
+        # exp-bound: the reference evaluates one exp per tap of its sum pass
+        # (N*(W+H) per image, ref_rate); the kernel skips taps whose terms lie
+        # below the sum's rounding, so achieved counts the exps it executed
+        mhz = peaks.get("sm_max_mhz", 1965.0)
+        ref_rate = N * (W + H) * imgs_per_launch / (conv_launch_ms * 1e-3) / 1e12
+        exec_rate = exps.value / max(conv_launches.value, 1) / (conv_launch_ms * 1e-3) / 1e12
+        peak = 148 * 16 * mhz * 1e6 / 1e12
+        roofline = dict(bound="sfu", achieved=exec_rate, peak=peak, unit="Texp/s",
+                        frac=exec_rate / peak, traffic=None,
+                        peak_source="of nominal MUFU peak (16 ex2 per SM per clock at max clock)",
+                        kernel=f"log-domain separable operator: one launch = {imgs_per_launch:.0f} images "
+                               "(two log-sum-exp axis passes)",
+                        reference_equivalent_texp_s=ref_rate,
+                        executed_exp_share=exps.value / max(conv_imgs.value * N * (W + H), 1),
+                        note="achieved = exps executed (counted on the device); the reference "
+                             "evaluates one per tap (reference_equivalent_texp_s); taps whose terms "
+                             "are provably below the sum's rounding are skipped",
+                        conv_share_of_step=conv_ms.value / (ms / args.steps))
+    elif precision in ("split_bf16", "tf32"):
         peak = peaks.get("bf16_tflops", 1590.0) * (0.5 if precision == "tf32" else 1.0)
         peak_src = "of measured bf16 burst" if peaks else "of fallback"
         bound = "tensor"
@@ -305,14 +363,15 @@ def run_ours(args):
         peak = 148 * 128 * 2 * mhz * 1e6 / 1e12 / (2.0 if precision == "fp64" else 1.0)
         peak_src = "of nominal CUDA-core FMA peak at max clock"
         bound = "fp32-cuda-core" if precision == "fp32" else "fp64-cuda-core"
-    roofline = dict(bound=bound, achieved=achieved_tflops, peak=peak, unit="TFLOP/s",
-                    frac=achieved_tflops / peak, traffic=None, peak_source=peak_src,
-                    executed_tflops=achieved_tflops * products,
-                    ceiling_frac=1.0 / products,
-                    kernel=(f"fused Sinkhorn kernel: one launch = {imgs_per_launch:.0f} separable-operator "
-                            "applications (whole forward + reverse pass)" if precision in ("split_bf16", "tf32")
-                            else f"separable Gaussian operator: one launch = {imgs_per_launch:.0f} images"),
-                    conv_share_of_step=conv_ms.value / (ms / args.steps))
+    if wl["domain"] != "log":
+        roofline = dict(bound=bound, achieved=achieved_tflops, peak=peak, unit="TFLOP/s",
+                        frac=achieved_tflops / peak, traffic=None, peak_source=peak_src,
+                        executed_tflops=achieved_tflops * products,
+                        ceiling_frac=1.0 / products,
+                        kernel=(f"fused Sinkhorn kernel: one launch = {imgs_per_launch:.0f} separable-operator "
+                                "applications (whole forward + reverse pass)" if precision in ("split_bf16", "tf32")
+                                else f"separable Gaussian operator: one launch = {imgs_per_launch:.0f} images"),
+                        conv_share_of_step=conv_ms.value / (ms / args.steps))
 
     # End to end through the public host-pointer API (pinned host buffers).
     e2e = None
@@ -350,13 +409,13 @@ def run_ours(args):
         e2e = dict(value=units / el, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h)
 
     serving = None
-    if rank == 0 and not args.no_serving:
+    if rank == 0 and not args.no_serving and wl["name"] == "batched128":
         serving = [run_serving(float(r), args.serve_requests, local)
                    for r in args.serve_rates.split(",") if r]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, _ = time_cpu_reference(steps=1, warmup=0)
+        cpu, _ = time_cpu_reference(wl, steps=1, warmup=0)
 
     if world > 1:
         torch.cuda.synchronize()
@@ -364,13 +423,14 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return
-    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+    line = dict(metric=metric_for(wl), value=value, unit=UNIT, n_gpus=world, steps=args.steps,
                 warmup=args.warmup, ms_per_step=ms / args.steps, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype=dtype_name(precision),
-                data="synthetic: seeded anisotropic Gaussian-blob histograms (2-5 blobs), "
+                data=f"synthetic: seeded anisotropic Gaussian-blob histograms ({wl['n_blobs'][0]}-"
+                     f"{wl['n_blobs'][1]} blobs, std {wl['std_frac'][0]}-{wl['std_frac'][1]} of the side), "
                      "uniform+noise atoms, U[0,1] weights",
-                config=dict(workload="batched128: P=64 per GPU, 128x128, K=5, L=100, gamma=1, KL loss",
-                            P_per_gpu=P, W=W, H=H, K=K, L=L, gamma=wl["gamma"], loss="KL",
+                config=dict(workload=describe(wl),
+                            P_per_gpu=P, W=W, H=H, K=K, L=L, gamma=wl["gamma"], loss=wl["loss_name"],
                             precision=precision, parallelism=f"dp{world} over histograms",
                             l2=f"working set larger than L2: iterate store {tape_gb:.2f} GB per GPU",
                             objective=fval),

@@ -162,6 +162,37 @@ typedef struct {
 } wdl_problem;
 int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* problems, int nproblems);
 
+/* ---- Batched weight fitting, L-BFGS on the device --------------------------------
+ * Fits the barycentric weights of every histogram of every problem onto the
+ * problem's fixed atoms: one L-BFGS per histogram over x in R^K with weights =
+ * softmax(x) (the reference's log-domain weights with scaleDictionary 1,
+ * cpp/inverseWasserstein.h:1000-1020, :1124-1133), liblbfgs' algorithm and
+ * constants as regress_both sets them (m = 6, strong-Wolfe backtracking, ftol
+ * 1e-4, wolfe 0.9, 20 trials; cpp/inverseWasserstein.h:362-372,
+ * cpp/lbfgs/lbfgs.c:256-654, :772-867), max_iterations accepted steps, stop
+ * when |g| / max(1, |x|) <= epsilon.  Every round evaluates all active
+ * histograms in one launch of the fused kernel (wdl_batch_run's layout) and
+ * advances every optimisation on the device; the round is a CUDA graph.
+ * Context as for wdl_batch_run.  status[p] is liblbfgs' return code, or
+ * WDL_FIT_OVERFLOW when the kernel-domain evaluation at the returned weights is
+ * not finite (scalings beyond the float range: run that histogram in the log
+ * domain).  loss[p] is the loss at the returned weights.  The reference's
+ * counterpart is regress_both with the atoms held fixed, one problem at a time
+ * on the host. */
+enum { WDL_FIT_OVERFLOW = -2000 };
+typedef struct {
+  int W, H, K, L, P, loss_type;
+  const double* atoms;     /* [K*N] fixed dictionary */
+  const double* observed;  /* [P*N] histograms to fit */
+  const double* x0;        /* [P*K] starting log-weights, or NULL (uniform weights) */
+  double* weights;         /* [P*K] out: fitted weights */
+  double* loss;            /* [P] out */
+  int* status;             /* [P] out */
+  int* evaluations;        /* [P] out: objective evaluations used */
+} wdl_fit_problem;
+int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* problems, int nproblems, int max_iterations,
+                    double epsilon);
+
 /* ---- Device-resident forms (device pointers, stream as void*) ----------------
  * Same semantics as the host forms; no host<->device copies, no synchronisation.
  * f is a device double. */
@@ -207,6 +238,10 @@ int wdl_set_profiling(wdl_ctx* ctx, int level);
 int wdl_phase_trace(wdl_ctx* ctx, double* out27);
 int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launches,
                      double* conv_images);
+/* Exponentials the log-domain operator evaluated while profiling (the
+ * reference evaluates one per tap, N*(W+H) per image; taps whose terms are
+ * below the sum's rounding are skipped here). */
+int wdl_exp_profile(const wdl_ctx* ctx, double* executed_exps);
 
 #ifdef __cplusplus
 }

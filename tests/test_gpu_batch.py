@@ -84,3 +84,83 @@ def test_uneven_weight_fitting(oracle):
         b0 = oracle.barycenter(W, H, 1, pr["gamma"], K, L, pr["atoms"].reshape(K, -1), np.ones(K) / K)
         f0, _ = oracle.loss(2, W, H, 1, pr["gamma"], b0, pr["observed"])
         assert f_ref <= f0 * (1 + 1e-6)
+
+
+def _host_fit(kern, pr, iters, eps):
+    """The same fit with the host L-BFGS (lbfgs_steps) around single-problem
+    batched evaluations: the reference's control flow, host side."""
+    from wassersteindictionarylearning_b200 import lbfgs as lb
+    from wassersteindictionarylearning_b200.batch import batch_run
+    K = pr["K"]
+    gen = lb.lbfgs_steps(np.zeros(K), lb.LbfgsParam(max_iterations=iters, epsilon=eps))
+    x = next(gen)
+    seen = {}
+    while True:
+        w = np.exp(x - x.max())
+        w /= w.sum()
+        o = batch_run(kern, [dict(W=pr["W"], H=pr["H"], K=K, L=pr["L"], P=1, atoms=pr["atoms"],
+                                  weights=w, observed=pr["observed"], loss_type=2)])[0]
+        f, la = float(o["loss"][0]), o["la"]
+        seen[x.tobytes()] = f
+        try:
+            x = gen.send((f, (la - np.dot(w, la)) * w))
+        except StopIteration as e:
+            st, xr, fx = e.value
+            wr = np.exp(xr - xr.max())
+            return wr / wr.sum(), seen.get(xr.tobytes(), fx), st
+
+
+def test_device_lbfgs_matches_host_lbfgs(oracle):
+    """wdl_fit_weights (L-BFGS on the device, graph-replayed rounds) takes the
+    decisions the host L-BFGS takes on the same evaluations."""
+    from wassersteindictionarylearning_b200 import CudaGaussian2DKernel
+    from wassersteindictionarylearning_b200.batch import fit_device
+    from wassersteindictionarylearning_b200.synthetic import blob_histograms
+    gamma = 1.5
+    probs = []
+    for i, (W, H, K, L, P) in enumerate([(32, 32, 3, 8, 2), (48, 40, 4, 6, 1), (64, 64, 5, 10, 2),
+                                         (40, 24, 3, 7, 1)]):
+        # blob atoms over a uniform half: the weights matter and the kernel
+        # domain stays in range
+        atoms = blob_histograms(K, W, H, seed=50 + i) + 1.0 / (W * H)
+        atoms /= atoms.sum(axis=1, keepdims=True)
+        probs.append(dict(W=W, H=H, K=K, L=L, loss_type=2, atoms=atoms.reshape(-1),
+                          observed=blob_histograms(P, W, H, seed=60 + i).reshape(-1)))
+    kern = CudaGaussian2DKernel(gamma, 128, 128, precision="split_bf16")
+    outs = fit_device(kern, probs, lbfgs_iterations=10, epsilon=1e-6)
+    for pr, (w, f, st, ev) in zip(probs, outs):
+        W, H, K, L = pr["W"], pr["H"], pr["K"], pr["L"]
+        N = W * H
+        obs = pr["observed"].reshape(-1, N)
+        for p in range(obs.shape[0]):
+            assert st[p] in (0, -997, -998) and ev[p] >= 3
+            assert abs(w[p].sum() - 1) < 1e-12 and (w[p] >= 0).all()
+            one = dict(pr, observed=obs[p])
+            wh, fh, sth = _host_fit(kern, one, 10, 1e-6)
+            assert abs(f[p] - fh) <= 1e-4 * abs(fh)
+            assert np.max(np.abs(w[p] - wh)) < 2e-3
+            # the reported loss is the FP64 oracle's at the returned weights
+            bary = oracle.barycenter(W, H, 1, gamma, K, L, pr["atoms"].reshape(K, N), w[p])
+            f_ref, _ = oracle.loss(2, W, H, 1, gamma, bary, obs[p])
+            assert abs(f[p] - f_ref) <= 1e-3 * abs(f_ref)
+            b0 = oracle.barycenter(W, H, 1, gamma, K, L, pr["atoms"].reshape(K, N), np.ones(K) / K)
+            f0, _ = oracle.loss(2, W, H, 1, gamma, b0, obs[p])
+            assert f_ref < f0
+    kern.close()
+
+
+def test_device_lbfgs_reports_overflow():
+    """Peaked atoms, gamma 2, 14 iterations: the FP32 kernel-domain scalings
+    leave the float range, and the device fit says so instead of returning a
+    NaN-driven result."""
+    from wassersteindictionarylearning_b200 import CudaGaussian2DKernel
+    from wassersteindictionarylearning_b200._lib import WDL_FIT_OVERFLOW
+    from wassersteindictionarylearning_b200.batch import fit_device
+    from wassersteindictionarylearning_b200.synthetic import blob_histograms
+    W = 32
+    pr = dict(W=W, H=W, K=4, L=14, loss_type=2, atoms=blob_histograms(4, W, W, seed=5).reshape(-1),
+              observed=blob_histograms(1, W, W, seed=6).reshape(-1))
+    kern = CudaGaussian2DKernel(2.0, 128, 128, precision="split_bf16")
+    (w, f, st, ev), = fit_device(kern, [pr], lbfgs_iterations=5)
+    kern.close()
+    assert st[0] == WDL_FIT_OVERFLOW and ev[0] == 1

@@ -30,6 +30,7 @@ _dp = C.POINTER(C.c_double)
 _vp = C.c_void_p
 
 WDL_MODE_WEIGHTS, WDL_MODE_BOTH, WDL_MODE_BARYCENTER = 0, 1, 2
+WDL_FIT_OVERFLOW = -2000
 
 
 class WdlProblem(C.Structure):
@@ -38,6 +39,14 @@ class WdlProblem(C.Structure):
                 ("loss_type", C.c_int), ("mode", C.c_int), ("atoms", _dp), ("weights", _dp),
                 ("observed", _dp), ("result_la", _dp), ("result_dic", _dp), ("bary", _dp),
                 ("loss", _dp)]
+
+
+class WdlFitProblem(C.Structure):
+    """struct wdl_fit_problem of include/wdl.h."""
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("K", C.c_int), ("L", C.c_int), ("P", C.c_int),
+                ("loss_type", C.c_int), ("atoms", _dp), ("observed", _dp), ("x0", _dp),
+                ("weights", _dp), ("loss", _dp), ("status", C.POINTER(C.c_int)),
+                ("evaluations", C.POINTER(C.c_int))]
 
 
 class WdlError(RuntimeError):
@@ -80,10 +89,12 @@ SIGNATURES = {
     "wdl_convolve_device": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
     "wdl_convolve_device_noalloc": ([_vp, _vp, _vp, C.c_int, _vp], C.c_int),
     "wdl_batch_run": ([_vp, C.c_void_p, C.c_int], C.c_int),
+    "wdl_fit_weights": ([_vp, C.c_void_p, C.c_int, C.c_int, C.c_double], C.c_int),
     "wdl_launch_count": ([_vp], C.c_longlong),
     "wdl_set_profiling": ([_vp, C.c_int], C.c_int),
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),
     "wdl_phase_trace": ([_vp, _dp], C.c_int),
+    "wdl_exp_profile": ([_vp, _dp], C.c_int),
 }
 
 _LIB = None

@@ -4,14 +4,17 @@ weight-fitting driver built on it.
 `batch_run` sends a list of problems (each its own grid side <= 128, K, L, P
 and mode) to one persistent launch of the fused tensor-core kernel.
 
-`fit_weights` fits the barycentric weights of many single histograms against
-their own fixed dictionaries (the weight half of regress_both with the atoms
-held fixed, cpp/inverseWasserstein.h:362-521, :635-673): every problem runs its
-own resumable L-BFGS (lbfgs.lbfgs_steps, liblbfgs' parameters); each round,
-all active problems of a gamma are evaluated in ONE batched launch on that
-gamma's context.  Problems with a side above 128 are evaluated on the FP32
-operator path of their own grid, and problems whose kernel-domain scalings
-overflow move to the log-domain operator.
+`fit_device` (wdl_fit_weights) fits the barycentric weights of many
+histograms against their own fixed dictionaries (the weight half of
+regress_both with the atoms held fixed, cpp/inverseWasserstein.h:362-521,
+:635-673) with the L-BFGS on the device: every round evaluates all active
+histograms of all problems in ONE launch and advances every optimisation in
+a second kernel, the round replayed as a CUDA graph.
+
+`fit_weights` is the uneven-workload driver around it: problems of sides up to
+128 go to the device per gamma; problems above the tile, and problems whose
+kernel-domain scalings overflow, are fitted with the host L-BFGS on the FP32
+operator path of their own grid, in the log domain where needed.
 """
 from __future__ import annotations
 
@@ -21,8 +24,8 @@ from collections import defaultdict
 import numpy as np
 
 from . import lbfgs as lb
-from ._lib import (WDL_MODE_BARYCENTER, WDL_MODE_BOTH, WDL_MODE_WEIGHTS, WdlProblem, check, dptr,
-                   f64, lib)
+from ._lib import (WDL_FIT_OVERFLOW, WDL_MODE_BARYCENTER, WDL_MODE_BOTH, WDL_MODE_WEIGHTS,
+                   WdlFitProblem, WdlProblem, check, dptr, f64, lib)
 from .kernels import CudaGaussian2DKernel, CudaLogSignArrayGaussian2DKernel
 
 MODES = {"weights": WDL_MODE_WEIGHTS, "both": WDL_MODE_BOTH, "barycenter": WDL_MODE_BARYCENTER}
@@ -59,105 +62,142 @@ def batch_run(kernel, problems):
     return outs
 
 
-def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0, max_side=128):
+def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6):
+    """wdl_fit_weights: every histogram of every problem fitted by its own
+    L-BFGS on the device, all evaluated together each round.  problems: dicts
+    with W, H, K, L, atoms [K*N], observed [P*N] (P = len / N), loss_type,
+    optional x0 [P*K].  Returns per problem (weights [P,K], loss [P], status
+    [P], evaluations [P])."""
+    n = len(problems)
+    arr = (WdlFitProblem * n)()
+    keep, outs = [], []
+    for i, pr in enumerate(problems):
+        W, H, K, L = (int(pr[k]) for k in ("W", "H", "K", "L"))
+        N = W * H
+        atoms = f64(pr["atoms"]).reshape(-1)
+        obs = f64(pr["observed"]).reshape(-1)
+        P = obs.size // N
+        x0 = None if pr.get("x0") is None else f64(pr["x0"]).reshape(-1)
+        w, f = np.empty(P * K), np.empty(P)
+        st, ev = np.empty(P, dtype=np.int32), np.empty(P, dtype=np.int32)
+        keep += [atoms, obs, x0]
+        outs.append((w, f, st, ev, P, K))
+        arr[i] = WdlFitProblem(W, H, K, L, P, int(pr.get("loss_type", 2)), dptr(atoms), dptr(obs),
+                               dptr(x0), dptr(w), dptr(f), st.ctypes.data_as(C.POINTER(C.c_int)),
+                               ev.ctypes.data_as(C.POINTER(C.c_int)))
+    check(lib().wdl_fit_weights(kernel.ctx, C.cast(arr, C.c_void_p), n, int(lbfgs_iterations),
+                                float(epsilon)), kernel.ctx)
+    return [(w.reshape(P, K), f, st, ev) for (w, f, st, ev, P, K) in outs]
+
+
+def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0, max_side=128,
+                epsilon=1e-6):
     """problems: dicts with W, H, K, L, gamma, atoms [K*N], observed [N],
     loss_type.  Returns per problem (weights [K], loss, lbfgs status,
     evaluations, domain).
 
-    Every problem starts in the kernel domain, batched per gamma.  The kernel
-    domain's scalings grow with the iterations wherever the atoms are nearly
-    empty (the dual potentials reach |d|^2 / gamma, far beyond any float range
-    for peaked atoms, a narrow kernel and long runs); a problem whose
-    evaluation comes back non-finite is moved, at the same point, to the
-    log-domain operator (the reference's LogSignArray kernels,
-    cpp/kernels.h:1034) and stays there."""
-    param = lb.LbfgsParam(max_iterations=lbfgs_iterations, epsilon=1e-6)
+    Problems whose side fits the tensor-core tile are fitted on the device,
+    all problems of a gamma in one wdl_fit_weights call (L-BFGS on the device,
+    one fused launch per round).  The kernel domain's scalings grow with the
+    iterations wherever the atoms are nearly empty (the dual potentials reach
+    |d|^2 / gamma, far beyond any float range for peaked atoms, a narrow kernel
+    and long runs); a problem whose kernel-domain evaluation comes back
+    non-finite is fitted again from its start in the log domain (the
+    reference's LogSignArray kernels, cpp/kernels.h:1034), with the host
+    L-BFGS (lbfgs.lbfgs_steps, liblbfgs' parameters) batched by rounds.
+    Problems with a side above the tile run on the FP32 operator path of their
+    own grid with the same escalation."""
+    results = [None] * len(problems)
+    host = []      # (index, starting domain, evaluations already spent)
+    by_gamma = defaultdict(list)
+    for i, pr in enumerate(problems):
+        if max(pr["W"], pr["H"]) <= max_side:
+            by_gamma[pr["gamma"]].append(i)
+        else:
+            host.append((i, "kernel", 0))
+    for g, idx in by_gamma.items():
+        kern = CudaGaussian2DKernel(g, max_side, max_side, precision=precision, device=device)
+        try:
+            outs = fit_device(kern, [problems[i] for i in idx], lbfgs_iterations, epsilon)
+        finally:
+            kern.close()
+        for i, (w, f, st, ev) in zip(idx, outs):
+            if int(st[0]) == WDL_FIT_OVERFLOW:
+                host.append((i, "log", int(ev[0])))
+            else:
+                results[i] = (w[0], float(f[0]), int(st[0]), int(ev[0]), "kernel")
+    if host:
+        for (i, _, spent), r in zip(host, _fit_host(problems, host, lbfgs_iterations, device,
+                                                    epsilon)):
+            w, f, st, ev, dom = r
+            results[i] = (w, f, st, ev + spent, dom)
+    return results
+
+
+def _fit_host(problems, todo, lbfgs_iterations, device, epsilon):
+    """Host L-BFGS per problem (resumable generator), every round's
+    evaluations issued problem by problem on the operator path of each
+    problem's grid: FP32 kernel domain, or the log domain."""
+    param = lb.LbfgsParam(max_iterations=lbfgs_iterations, epsilon=epsilon)
     states = []
-    for pr in problems:
-        gen = lb.lbfgs_steps(np.zeros(int(pr["K"])), param)
-        states.append({"gen": gen, "x": next(gen), "done": False, "evals": 0, "seen": {},
-                       "domain": "kernel"})
+    for i, dom, _ in todo:
+        gen = lb.lbfgs_steps(np.zeros(int(problems[i]["K"])), param)
+        states.append({"i": i, "gen": gen, "x": next(gen), "done": False, "evals": 0, "seen": {},
+                       "domain": dom})
     ctxs = {}
 
     def ctx_for(key):
         if key not in ctxs:
             kind, W, H, g = key
-            if kind == "tc":
-                ctxs[key] = CudaGaussian2DKernel(g, W, H, precision=precision, device=device)
-            elif kind == "kernel":
+            if kind == "kernel":
                 ctxs[key] = CudaGaussian2DKernel(g, W, H, precision="fp32", device=device)
             else:
                 ctxs[key] = CudaLogSignArrayGaussian2DKernel(g, W, H, precision="fp32", device=device)
         return ctxs[key]
 
-    results = [None] * len(problems)
-    while True:
-        active = [i for i, s in enumerate(states) if not s["done"]]
-        if not active:
-            break
-        groups = defaultdict(list)
-        for i in active:
-            pr = problems[i]
-            if states[i]["domain"] == "log":
-                key = ("log", pr["W"], pr["H"], pr["gamma"])
-            elif max(pr["W"], pr["H"]) > max_side:
-                key = ("kernel", pr["W"], pr["H"], pr["gamma"])
-            else:
-                key = ("tc", max_side, max_side, pr["gamma"])
-            groups[key].append(i)
-        evals = {}
-        for key, idx in groups.items():
-            lam = {}
-            batch = []
-            for i in idx:
-                x = states[i]["x"]
+    results = [None] * len(states)
+    try:
+        while True:
+            active = [j for j, s in enumerate(states) if not s["done"]]
+            if not active:
+                break
+            for j in active:
+                s = states[j]
+                pr = problems[s["i"]]
+                kern = ctx_for((s["domain"], pr["W"], pr["H"], pr["gamma"]))
+                x = s["x"]
                 w = np.exp(x - x.max())
-                lam[i] = w / w.sum()
-                pr = problems[i]
-                batch.append(dict(W=pr["W"], H=pr["H"], K=pr["K"], L=pr["L"], P=1, atoms=pr["atoms"],
-                                  weights=lam[i], observed=pr["observed"],
-                                  loss_type=pr.get("loss_type", 2), mode="weights"))
-            kern = ctx_for(key)
-            if key[0] == "tc":
-                outs = batch_run(kern, batch)
-            else:  # one problem per call on the operator path of its own grid
-                outs = []
-                for b in batch:
-                    K, N = b["K"], b["W"] * b["H"]
-                    la, dic, loss = np.empty(K), np.empty(K * N), np.empty(1)
-                    check(lib().wdl_gradient_both(kern.ctx, 1, K, b["L"], b["loss_type"],
-                                                  dptr(f64(b["atoms"])), dptr(f64(b["weights"])),
-                                                  dptr(f64(b["observed"])), None, dptr(la),
-                                                  dptr(dic), None, dptr(loss), None), kern.ctx)
-                    outs.append({"la": la, "loss": loss})
-            for i, o in zip(idx, outs):
-                evals[i] = (o, lam[i])
-        for i, (o, w) in evals.items():
-            s = states[i]
-            la = o["la"]
-            f = float(o["loss"][0])
-            finite = np.isfinite(f) and np.all(np.isfinite(la))
-            if not finite and s["domain"] == "kernel":
-                s["domain"] = "log"  # re-evaluate the same point next round
-                continue
-            s["evals"] += 1
-            g = (la - np.dot(w, la)) * w
-            if not finite:
-                f, g = float("inf"), np.zeros_like(g)
-            s["seen"][s["x"].tobytes()] = f
-            try:
-                s["x"] = s["gen"].send((f, g))
-            except StopIteration as e:
-                # a failed line search returns the last accepted point with
-                # the last TRIAL value (as liblbfgs does): report the loss
-                # evaluated at the point returned
-                status, x, fx = e.value
-                w = np.exp(x - x.max())
-                results[i] = (w / w.sum(), s["seen"].get(x.tobytes(), fx), status, s["evals"],
-                              s["domain"])
-                s["done"] = True
-    for k in ctxs.values():
-        k.close()
+                w /= w.sum()
+                K, N = int(pr["K"]), pr["W"] * pr["H"]
+                la, dic, loss = np.empty(K), np.empty(K * N), np.empty(1)
+                check(lib().wdl_gradient_both(kern.ctx, 1, K, int(pr["L"]), int(pr.get("loss_type", 2)),
+                                              dptr(f64(pr["atoms"])), dptr(w), dptr(f64(pr["observed"])),
+                                              None, dptr(la), dptr(dic), None, dptr(loss), None),
+                      kern.ctx)
+                f = float(loss[0])
+                finite = np.isfinite(f) and np.all(np.isfinite(la))
+                if not finite and s["domain"] == "kernel":
+                    s["domain"] = "log"  # re-evaluate the same point next round
+                    continue
+                s["evals"] += 1
+                g = (la - np.dot(w, la)) * w
+                if not finite:
+                    f, g = float("inf"), np.zeros_like(g)
+                s["seen"][x.tobytes()] = f
+                try:
+                    s["x"] = s["gen"].send((f, g))
+                except StopIteration as e:
+                    # a failed line search returns the last accepted point with
+                    # the last TRIAL value (as liblbfgs does): report the loss
+                    # evaluated at the point returned
+                    status, xr, fx = e.value
+                    wr = np.exp(xr - xr.max())
+                    results[j] = (wr / wr.sum(), s["seen"].get(xr.tobytes(), fx), status, s["evals"],
+                                  s["domain"])
+                    s["done"] = True
+    finally:
+        for k in ctxs.values():
+            k.close()
     return results
 
 

@@ -249,6 +249,7 @@ int wdl_destroy(wdl_ctx* ctx) {
   }
   if (ctx->arena.ptr) cudaFree(ctx->arena.ptr);
   if (ctx->d_trace) cudaFree(ctx->d_trace);
+  if (ctx->d_taps) cudaFree(ctx->d_taps);
   if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
   if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -276,6 +277,7 @@ int wdl_set_profiling(wdl_ctx* ctx, int on) {
   ctx->conv_ms = 0;
   ctx->conv_launches = 0;
   ctx->conv_images = 0;
+  ctx->log_exps = 0;
   return WDL_OK;
 }
 
@@ -287,6 +289,12 @@ int wdl_phase_trace(wdl_ctx* ctx, double* out27) {
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   WDL_CUDA_TRY(ctx, cudaMemcpy(h, ctx->d_trace, sizeof(h), cudaMemcpyDeviceToHost));
   for (int i = 0; i < 27; ++i) out27[i] = (double)h[i];
+  return WDL_OK;
+}
+
+int wdl_exp_profile(const wdl_ctx* ctx, double* executed_exps) {
+  if (!ctx || !executed_exps) return WDL_ERR_INVALID_ARG;
+  *executed_exps = ctx->log_exps;
   return WDL_OK;
 }
 

@@ -96,16 +96,13 @@ struct Carve {
 };
 
 }  // namespace
-}  // namespace wdl
 
-using namespace wdl;
-
-extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
+int batch_prepare(wdl_ctx* ctx, const wdl_problem* pb, int nprob, size_t extra_bytes, BatchPlan& bp,
+                  cudaStream_t s) {
   if (!ctx || !pb || nprob < 1) return set_error(ctx, WDL_ERR_INVALID_ARG, "bad arguments");
   if (!ctx->tc || ctx->domain != WDL_DOMAIN_KERNEL)
     return set_error(ctx, WDL_ERR_UNSUPPORTED,
-                     "wdl_batch_run needs a kernel-domain WDL_TF32 or WDL_SPLIT_BF16 context");
-  cudaSetDevice(ctx->device);
+                     "many-problem launches need a kernel-domain WDL_TF32 or WDL_SPLIT_BF16 context");
   const bool split = ctx->precision == WDL_SPLIT_BF16;
   for (int q = 0; q < nprob; ++q) {
     const wdl_problem& w = pb[q];
@@ -118,32 +115,23 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
       return set_error(ctx, WDL_ERR_INVALID_ARG,
                        "problem " + std::to_string(q) + ": needs observations and loss 1, 2 or 4");
   }
+  bp.nprob = nprob;
+  bp.buf.assign(nprob, BatchBuf{});
+  bp.prs.assign(nprob, SkProblem{});
   // ---- layout: one arena region per problem, all in one allocation ----------------
-  struct Off {
-    double *atoms64, *lam64, *dot, *loss, *obs, *in_atoms, *in_w, *out_la, *out_loss, *out_bary,
-        *out_dic;
-    float *atoms, *lam, *cb, *phi, *acc, *nb, *gwb, *v, *r, *gdic;
-    int* sync;
-  };
-  std::vector<Off> off(nprob);
-  std::vector<SkProblem> prs(nprob);
-  struct Marks {
-    size_t probs, gsync, zero_b, zero_e, in_b, in_e, out_b, out_e, total;
-  };
   auto plan = [&](char* basep) {
-    Marks m{};
     Carve c{basep};
-    m.probs = c.mark();
+    bp.probs = c.mark();
     c.take<SkProblem>(nprob);
-    m.gsync = c.mark();
+    bp.gsync = c.mark();
     c.take<int>(2);
-    m.zero_b = c.mark();  // region that must start at zero
+    bp.zero_b = c.mark();  // region that must start at zero
     for (int q = 0; q < nprob; ++q) {
       const wdl_problem& w = pb[q];
       const size_t N = (size_t)w.W * w.H, P = w.P, K = w.K, L = w.L;
       const bool fo = w.mode == WDL_MODE_BARYCENTER, dic = w.mode == WDL_MODE_BOTH;
       const size_t slots = fo ? 2 : L;
-      Off& o = off[q];
+      BatchBuf& o = bp.buf[q];
       o.acc = c.take<float>(slots * P * N);
       o.dot = c.take<double>(P * K);
       o.nb = c.take<float>(dic ? 2 * P * N : 1);
@@ -152,13 +140,13 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
       o.r = c.take<float>(fo ? 1 : P * K * N);
       o.gdic = c.take<float>(dic ? P * K * N : 1);
     }
-    m.zero_e = c.mark();
+    bp.zero_e = c.mark();
     for (int q = 0; q < nprob; ++q) {
       const wdl_problem& w = pb[q];
       const size_t N = (size_t)w.W * w.H, P = w.P, K = w.K, L = w.L;
       const bool fo = w.mode == WDL_MODE_BARYCENTER;
       const size_t slots = fo ? 2 : L;
-      Off& o = off[q];
+      BatchBuf& o = bp.buf[q];
       o.atoms64 = c.take<double>(K * N);
       o.lam64 = c.take<double>(P * K);
       o.loss = c.take<double>(P);
@@ -168,72 +156,74 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
       o.phi = c.take<float>(slots * P * K * N);
       o.sync = c.take<int>(4 * P);
     }
-    m.in_b = c.mark();  // inputs: one upload
+    bp.in_b = c.mark();  // inputs: one upload
     for (int q = 0; q < nprob; ++q) {
       const wdl_problem& w = pb[q];
       const size_t N = (size_t)w.W * w.H;
-      off[q].in_atoms = c.take<double>((size_t)w.K * N);
-      off[q].in_w = c.take<double>((size_t)w.P * w.K);
-      off[q].obs = w.mode == WDL_MODE_BARYCENTER ? nullptr : c.take<double>((size_t)w.P * N);
+      bp.buf[q].in_atoms = c.take<double>((size_t)w.K * N);
+      bp.buf[q].in_w = c.take<double>((size_t)w.P * w.K);
+      bp.buf[q].obs = w.mode == WDL_MODE_BARYCENTER ? nullptr : c.take<double>((size_t)w.P * N);
     }
-    m.in_e = c.mark();
-    m.out_b = m.in_e;  // outputs: one download
+    bp.in_e = c.mark();
+    bp.out_b = bp.in_e;  // outputs: one download
     for (int q = 0; q < nprob; ++q) {
       const wdl_problem& w = pb[q];
       const size_t N = (size_t)w.W * w.H;
       const bool grad = w.mode != WDL_MODE_BARYCENTER;
-      off[q].out_la = (grad && w.result_la) ? c.take<double>((size_t)w.P * w.K) : nullptr;
-      off[q].out_loss = (grad && w.loss) ? c.take<double>((size_t)w.P) : nullptr;
-      off[q].out_bary = w.bary ? c.take<double>((size_t)w.P * N) : nullptr;
-      off[q].out_dic = (w.mode == WDL_MODE_BOTH && w.result_dic) ? c.take<double>((size_t)w.K * N) : nullptr;
+      BatchBuf& o = bp.buf[q];
+      o.out_la = (grad && w.result_la) ? c.take<double>((size_t)w.P * w.K) : nullptr;
+      o.out_loss = (grad && w.loss) ? c.take<double>((size_t)w.P) : nullptr;
+      o.out_bary = w.bary ? c.take<double>((size_t)w.P * N) : nullptr;
+      o.out_dic = (w.mode == WDL_MODE_BOTH && w.result_dic) ? c.take<double>((size_t)w.K * N) : nullptr;
     }
-    m.out_e = c.mark();
-    m.total = m.out_e;
-    return m;
+    bp.out_e = c.mark();
+    return c.off;
   };
-  const Marks sz = plan(nullptr);
-  size_t n_rows = 0, n_out = 0, n_items = 0;
+  const size_t core = plan(nullptr);
+  size_t n_rows = 0;
+  bp.n_outjobs = 0;
+  bp.n_items_all = 0;
   for (int q = 0; q < nprob; ++q) {
     const wdl_problem& w = pb[q];
     const bool grad = w.mode != WDL_MODE_BARYCENTER;
     n_rows += (size_t)w.K + w.P;
-    n_out += (w.bary ? 1 : 0) + (w.mode == WDL_MODE_BOTH && w.result_dic ? 1 : 0) +
-             (grad && w.result_la ? 1 : 0) + (grad && w.loss ? 1 : 0);
+    bp.n_outjobs += (w.bary ? 1 : 0) + (w.mode == WDL_MODE_BOTH && w.result_dic ? 1 : 0) +
+                    (grad && w.result_la ? 1 : 0) + (grad && w.loss ? 1 : 0);
     SkProblem tmp{};
     tmp.K = w.K;
     tmp.L = w.L;
     tmp.P = w.P;
     tmp.fwd_only = w.mode == WDL_MODE_BARYCENTER;
     tmp.need_dic = w.mode == WDL_MODE_BOTH;
-    n_items += sk_problem_items(tmp);
+    bp.n_items_all += sk_problem_items(tmp);
   }
-  if (n_items > 0x7fffffff) return set_error(ctx, WDL_ERR_INVALID_ARG, "too many work items");
-  const size_t rows_off = sz.total;
-  const size_t out_off = r256(rows_off + n_rows * sizeof(RowJob));
-  const size_t items_off = r256(out_off + n_out * sizeof(OutJob));
-  const size_t need = items_off + n_items * sizeof(int4) + 256;
+  if (bp.n_items_all > 0x7fffffff) return set_error(ctx, WDL_ERR_INVALID_ARG, "too many work items");
+  bp.rows_off = r256(core);
+  bp.outj_off = r256(bp.rows_off + n_rows * sizeof(RowJob));
+  bp.items_off = r256(bp.outj_off + bp.n_outjobs * sizeof(OutJob));
+  bp.extra_off = r256(bp.items_off + bp.n_items_all * sizeof(int4));
   int rc;
-  if ((rc = ensure_arena(ctx, need))) return rc;
+  if ((rc = ensure_arena(ctx, bp.extra_off + extra_bytes + 256))) return rc;
   char* base = static_cast<char*>(ctx->arena.ptr);
+  bp.base = base;
   plan(base);
-  cudaStream_t s = ctx->stream;
+  bp.sync = reinterpret_cast<int*>(base + bp.gsync);
 
   // ---- host tables ----------------------------------------------------------------
-  std::vector<char> h_in(sz.in_e - sz.in_b);
+  std::vector<char> h_in(bp.in_e - bp.in_b);
   std::vector<RowJob> rows;
   rows.reserve(n_rows);
   std::vector<OutJob> outs;
-  int rounds_max = 0;
   for (int q = 0; q < nprob; ++q) {
     const wdl_problem& w = pb[q];
     const size_t N = (size_t)w.W * w.H;
-    Off& o = off[q];
-    std::memcpy(h_in.data() + ((char*)o.in_atoms - base - sz.in_b), w.atoms, (size_t)w.K * N * 8);
-    std::memcpy(h_in.data() + ((char*)o.in_w - base - sz.in_b), w.weights, (size_t)w.P * w.K * 8);
-    if (o.obs) std::memcpy(h_in.data() + ((char*)o.obs - base - sz.in_b), w.observed, (size_t)w.P * N * 8);
+    BatchBuf& o = bp.buf[q];
+    std::memcpy(h_in.data() + ((char*)o.in_atoms - base - bp.in_b), w.atoms, (size_t)w.K * N * 8);
+    std::memcpy(h_in.data() + ((char*)o.in_w - base - bp.in_b), w.weights, (size_t)w.P * w.K * 8);
+    if (o.obs) std::memcpy(h_in.data() + ((char*)o.obs - base - bp.in_b), w.observed, (size_t)w.P * N * 8);
     for (int k = 0; k < w.K; ++k) rows.push_back({o.in_atoms + k * N, o.atoms64 + k * N, o.atoms + k * N, (int)N});
     for (int p = 0; p < w.P; ++p) rows.push_back({o.in_w + (size_t)p * w.K, o.lam64 + (size_t)p * w.K, o.lam + (size_t)p * w.K, w.K});
-    SkProblem& pr = prs[q];
+    SkProblem& pr = bp.prs[q];
     pr = SkProblem{};
     sk_fill_geometry(pr, w.W, w.H, split);
     pr.K = w.K;
@@ -257,8 +247,6 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
     pr.dot = o.dot;
     pr.loss = o.loss;
     pr.sync = o.sync;
-    const int rounds = pr.fwd_only ? w.L : 2 * w.L;
-    if (rounds > rounds_max) rounds_max = rounds;
     if (o.out_bary)
       outs.push_back({0, w.P, o.acc + (size_t)(pr.fwd_only ? ((w.L - 1) & 1) : (w.L - 1)) * w.P * N,
                       nullptr, o.out_bary, (size_t)w.P * N});
@@ -266,62 +254,95 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
     if (o.out_la) outs.push_back({2, w.P, nullptr, o.dot, o.out_la, (size_t)w.P * w.K});
     if (o.out_loss) outs.push_back({2, w.P, nullptr, o.loss, o.out_loss, (size_t)w.P});
   }
-  // Work items by round: forward iterations, then reverse steps, every problem
-  // interleaved so that all dependency chains advance together.
-  std::vector<int4> items;
-  items.reserve(n_items);
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.in_b, h_in.data(), h_in.size(), cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.rows_off, rows.data(), rows.size() * sizeof(RowJob), cudaMemcpyHostToDevice, s));
+  if (!outs.empty())
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.outj_off, outs.data(), outs.size() * sizeof(OutJob), cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.probs, bp.prs.data(), bp.prs.size() * sizeof(SkProblem), cudaMemcpyHostToDevice, s));
+  k_rows<<<grid_for(rows.size(), 1, ctx->sm_count, 4), 256, 0, s>>>(reinterpret_cast<RowJob*>(base + bp.rows_off), (int)rows.size());
+  WDL_LAUNCH_CHECK(ctx);
+  // the error word is cleared here once; every launch clears only the counter
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(bp.sync, 0, 2 * sizeof(int), s));
+  // host copies must outlive the asynchronous uploads
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return WDL_OK;
+}
+
+void batch_items(const BatchPlan& bp, const std::vector<uint8_t>* active, std::vector<int4>& items) {
+  items.clear();
+  std::vector<size_t> first(bp.nprob + 1, 0);
+  int rounds_max = 0;
+  for (int q = 0; q < bp.nprob; ++q) {
+    first[q + 1] = first[q] + bp.prs[q].P;
+    const int rounds = bp.prs[q].fwd_only ? bp.prs[q].L : 2 * bp.prs[q].L;
+    if (rounds > rounds_max) rounds_max = rounds;
+  }
   for (int r = 0; r < rounds_max; ++r) {
-    for (int q = 0; q < nprob; ++q) {
-      const SkProblem& pr = prs[q];
+    for (int q = 0; q < bp.nprob; ++q) {
+      const SkProblem& pr = bp.prs[q];
       const int PK = pr.P * pr.K;
       if (r < pr.L) {
-        for (int pk = 0; pk < PK; ++pk) items.push_back(make_int4(q, 0, r + 1, pk));
+        for (int pk = 0; pk < PK; ++pk)
+          if (!active || (*active)[first[q] + pk / pr.K]) items.push_back(make_int4(q, 0, r + 1, pk));
       } else if (!pr.fwd_only && r < 2 * pr.L) {
         const int sstep = 2 * pr.L - r;
         for (int pk = 0; pk < PK; ++pk) {
+          if (active && !(*active)[first[q] + pk / pr.K]) continue;
           if (pr.need_dic) items.push_back(make_int4(q, 1, sstep, pk));
           items.push_back(make_int4(q, 2, sstep, pk));
         }
       }
     }
   }
-  if (items.size() != n_items) return set_error(ctx, WDL_ERR_INVALID_ARG, "internal: item count mismatch");
+}
 
-  // ---- device work ------------------------------------------------------------------
-  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + sz.in_b, h_in.data(), h_in.size(), cudaMemcpyHostToDevice, s));
-  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + rows_off, rows.data(), rows.size() * sizeof(RowJob), cudaMemcpyHostToDevice, s));
-  if (!outs.empty())
-    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + out_off, outs.data(), outs.size() * sizeof(OutJob), cudaMemcpyHostToDevice, s));
-  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + items_off, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
-  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + sz.probs, prs.data(), prs.size() * sizeof(SkProblem), cudaMemcpyHostToDevice, s));
-  WDL_CUDA_TRY(ctx, cudaMemsetAsync(base + sz.zero_b, 0, sz.zero_e - sz.zero_b, s));
-  k_rows<<<grid_for(rows.size(), 1, ctx->sm_count, 4), 256, 0, s>>>(reinterpret_cast<RowJob*>(base + rows_off), (int)rows.size());
-  WDL_LAUNCH_CHECK(ctx);
+int batch_launch(wdl_ctx* ctx, BatchPlan& bp, size_t n_items, cudaStream_t s) {
+  char* base = bp.base;
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(base + bp.zero_b, 0, bp.zero_e - bp.zero_b, s));
   SkArgs a{};
   a.G = ctx->G32[ctx->W >= ctx->H ? 0 : 1];
   a.Gn = ctx->W >= ctx->H ? ctx->W : ctx->H;
-  a.nprobs = nprob;
-  a.probs = reinterpret_cast<SkProblem*>(base + sz.probs);
-  a.items = reinterpret_cast<int4*>(base + items_off);
+  a.nprobs = bp.nprob;
+  a.probs = reinterpret_cast<SkProblem*>(base + bp.probs);
+  a.items = reinterpret_cast<int4*>(base + bp.items_off);
   a.total = (long long)n_items;
-  for (int q = 0; q < nprob; ++q) a.apps += sk_problem_applications(prs[q]);
-  a.sync = reinterpret_cast<int*>(base + sz.gsync);
-  if ((rc = sinkhorn_tc_launch(ctx, a, s))) return rc;
-  ctx->fused_sync = a.sync;
-  if (!outs.empty()) {
-    k_outputs<<<grid_for(outs.size(), 1, ctx->sm_count, 4), 256, 0, s>>>(reinterpret_cast<OutJob*>(base + out_off), (int)outs.size());
+  for (int q = 0; q < bp.nprob; ++q) a.apps += sk_problem_applications(bp.prs[q]);
+  a.sync = bp.sync;
+  return sinkhorn_tc_launch(ctx, a, s);
+}
+
+}  // namespace wdl
+
+using namespace wdl;
+
+extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(ctx, WDL_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = ctx->stream;
+  BatchPlan bp;
+  int rc;
+  if ((rc = batch_prepare(ctx, pb, nprob, 0, bp, s))) return rc;
+  std::vector<int4> items;
+  batch_items(bp, nullptr, items);
+  if (items.size() != bp.n_items_all) return set_error(ctx, WDL_ERR_INVALID_ARG, "internal: item count mismatch");
+  char* base = bp.base;
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.items_off, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  if ((rc = batch_launch(ctx, bp, items.size(), s))) return rc;
+  ctx->fused_sync = bp.sync;
+  if (bp.n_outjobs) {
+    k_outputs<<<grid_for(bp.n_outjobs, 1, ctx->sm_count, 4), 256, 0, s>>>(reinterpret_cast<OutJob*>(base + bp.outj_off), (int)bp.n_outjobs);
     WDL_LAUNCH_CHECK(ctx);
   }
   // ---- results: one download, scattered on the host --------------------------------
-  std::vector<char> h_out(sz.out_e - sz.out_b);
+  std::vector<char> h_out(bp.out_e - bp.out_b);
   if (!h_out.empty())
-    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), base + sz.out_b, h_out.size(), cudaMemcpyDeviceToHost, s));
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), base + bp.out_b, h_out.size(), cudaMemcpyDeviceToHost, s));
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-  auto host_of = [&](const double* d) { return h_out.data() + ((const char*)d - base - sz.out_b); };
+  auto host_of = [&](const double* d) { return h_out.data() + ((const char*)d - base - bp.out_b); };
   for (int q = 0; q < nprob; ++q) {
     const wdl_problem& w = pb[q];
     const size_t N = (size_t)w.W * w.H;
-    const Off& o = off[q];
+    const BatchBuf& o = bp.buf[q];
     if (o.out_la) std::memcpy(w.result_la, host_of(o.out_la), (size_t)w.P * w.K * 8);
     if (o.out_loss) std::memcpy(w.loss, host_of(o.out_loss), (size_t)w.P * 8);
     if (o.out_bary) std::memcpy(w.bary, host_of(o.out_bary), (size_t)w.P * N * 8);

@@ -136,7 +136,8 @@ struct LogOps<double> {
 template <typename T, bool SIGNED>
 __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
-    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign) {
+    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
+    unsigned long long* __restrict__ exps) {
   using Op = LogOps<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int CP = C + 1;                                 // odd row stride (elements)
@@ -173,11 +174,13 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
   for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d) * T(d) / gamma_t * Op::kScale;
   __syncthreads();
   // Thread -> (c, rr) with rr fastest so that stores out[c][r0+rr] are contiguous.
+  unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
   for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
     const int c = e / LR, rr = e - c * LR;
     if (rr >= nr) continue;
     const T* row = rows + rr * CP;
     const T X = xmax[rr];
+    int dmax = 0;
     T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
     for (int d = 1; d < C; ++d) {
       const T l = lk[d];
@@ -192,6 +195,7 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     for (int d = 1; d < C; ++d) {
       const T l = lk[d];
       if (l + X < floor_) break;
+      dmax = d;
       const T lm = l - m;
       if (c - d >= 0) {
         const T ex = Op::ex(lm + row[c - d]);
@@ -209,6 +213,13 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     } else {
       out[o] = (Op::lg(sum) + m) * Op::kUnscale;
     }
+    n_ex += 1 + min(dmax, c) + min(dmax, C - 1 - c);
+  }
+  if (exps) {
+    unsigned long long v = n_ex;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(exps, v);
   }
 }
 
@@ -227,11 +238,12 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
       auto k = log_axis_pass_kernel<T, true>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
-                                out_sign + off);
+                                out_sign + off, ctx->profiling ? ctx->d_taps : nullptr);
     } else {
       auto k = log_axis_pass_kernel<T, false>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr);
+      k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr,
+                                ctx->profiling ? ctx->d_taps : nullptr);
     }
     WDL_LAUNCH_CHECK(ctx);
     done += chunk;
@@ -250,8 +262,18 @@ struct ConvTimer {
   wdl_ctx* ctx;
   cudaStream_t s;
   size_t nimg;
-  ConvTimer(wdl_ctx* c, cudaStream_t st, size_t n) : ctx(c), s(st), nimg(n) {
-    if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
+  bool count_exps;
+  ConvTimer(wdl_ctx* c, cudaStream_t st, size_t n, bool exps = false)
+      : ctx(c), s(st), nimg(n), count_exps(exps && c->profiling) {
+    if (!ctx->profiling) return;
+    if (count_exps) {
+      if (!ctx->d_taps && cudaMalloc(&ctx->d_taps, sizeof(unsigned long long)) != cudaSuccess) {
+        ctx->d_taps = nullptr;
+        count_exps = false;
+      }
+      if (count_exps) cudaMemsetAsync(ctx->d_taps, 0, sizeof(unsigned long long), s);
+    }
+    cudaEventRecord(ctx->ev_a, s);
   }
   void done() {
     if (!ctx->profiling) return;
@@ -262,6 +284,11 @@ struct ConvTimer {
     ctx->conv_ms += ms;
     ctx->conv_launches += 1;
     ctx->conv_images += (double)nimg;
+    if (count_exps) {
+      unsigned long long h = 0;
+      if (cudaMemcpy(&h, ctx->d_taps, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess)
+        ctx->log_exps += (double)h;
+    }
   }
 };
 
@@ -291,7 +318,7 @@ int log_conv_stack_simt(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg,
     return set_error(ctx, WDL_ERR_UNSUPPORTED, "log-domain operator is 2-D only (as the reference)");
   const int W = ctx->W, H = ctx->H;
   const size_t N = ctx->N;
-  ConvTimer timer(ctx, s, nimg);
+  ConvTimer timer(ctx, s, nimg, true);
   int rc;
   if ((rc = log_axis_pass<T>(ctx, in, tmp, H, W, nimg, N, in_sign, in_sign ? tmp_sign : nullptr, s)))
     return rc;

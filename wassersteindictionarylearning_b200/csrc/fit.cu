@@ -1,0 +1,440 @@
+// wdl_fit_weights: batched weight fitting (projection onto fixed dictionaries)
+// with the L-BFGS outer loop on the device.
+//
+// The reference fits weights with liblbfgs on the host around evaluate_both
+// (regress_both, cpp/inverseWasserstein.h:362-423; lbfgs.c:256-654 with the
+// strong-Wolfe backtracking line search of lbfgs.c:772-867).  Here every
+// histogram of every problem is one optimisation whose state (x, g, the
+// previous point, the direction, m = 6 correction pairs) lives in device
+// memory.  One round is: the fused kernel evaluates every active histogram at
+// its current trial point (many problems per launch, wdl_batch_run's layout),
+// then k_fit_round consumes each loss and weight gradient and advances that
+// optimisation's state machine to its next trial point.  The round is captured
+// once in a CUDA graph and replayed; the host only looks at the done flags
+// every few rounds to drop finished histograms from the item table.
+//
+// Variables: x in R^K per histogram, weights = softmax(x) (the reference's
+// exp_weight transform with scaleDictionary 1 followed by the normalisation
+// by the sum, cpp/inverseWasserstein.h:1000-1020); gradient =
+// (la - <w, la>) * w, the projection and chain rule of evaluate_both
+// (:1092-1097, :1124-1133).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "wdl_internal.cuh"
+
+namespace wdl {
+namespace {
+
+constexpr int kM = 6;  // correction pairs (liblbfgs default, kept by the reference)
+
+// liblbfgs return codes (cpp/lbfgs/lbfgs.h:74-147)
+constexpr int kSuccess = 0, kAlreadyMinimized = 2, kMinimumStep = -1000, kMaximumStep = -999,
+              kMaximumLinesearch = -998, kMaximumIteration = -997, kInvalidParameters = -995,
+              kIncreaseGradient = -994;
+
+struct LbParam {
+  int max_iterations, max_linesearch;
+  double epsilon, ftol, wolfe, min_step, max_step;
+};
+
+struct LbOpt {
+  int K, phase;  // phase: 0 first evaluation pending, 1 line-search trial pending, 2 done
+  int k, end, count, status, evals;
+  double f, finit, dginit, step, fret;
+  double* v;            // x, g, xp, gp, d [K each], s[m][K], y[m][K], ys[m], alpha[m]
+  double* lam64;        // the weights the fused kernel evaluates ([K], FP64 and FP32)
+  float* lam32;
+  const double* dot;    // weight gradient of that evaluation ([K], raw resultLa)
+  const double* loss;   // its loss
+};
+
+inline size_t pool_doubles(int K) { return (size_t)(5 + 2 * kM) * K + 2 * kM; }
+
+__device__ void put_weights(const LbOpt& o, const double* x) {
+  double mx = x[0];
+  for (int k = 1; k < o.K; ++k) mx = x[k] > mx ? x[k] : mx;
+  double s = 0;
+  for (int k = 0; k < o.K; ++k) s += exp(x[k] - mx);
+  for (int k = 0; k < o.K; ++k) {
+    const double w = exp(x[k] - mx) / s;
+    o.lam64[k] = w;
+    o.lam32[k] = (float)w;
+  }
+}
+
+__device__ double dotk(const double* a, const double* b, int K) {
+  double s = 0;
+  for (int k = 0; k < K; ++k) s += a[k] * b[k];
+  return s;
+}
+
+__global__ void k_fit_init(LbOpt* opts, int n, const double* x0s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  LbOpt o = opts[i];
+  double* x = o.v;
+  for (int k = 0; k < o.K; ++k) x[k] = x0s ? x0s[(size_t)i * 64 + k] : 0.0;
+  put_weights(o, x);
+}
+
+// One optimisation step per histogram: consume the evaluation at the current
+// trial point, move to the next trial point (or finish).  Same decisions, in
+// the same order, as lbfgs_steps / liblbfgs.
+__global__ void k_fit_round(LbOpt* opts, int n, LbParam prm, const int* fused_sync, int* sticky,
+                            uint8_t* done) {
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = *(volatile const int*)(fused_sync + 1);
+  __syncthreads();
+  if (s_err) {  // the evaluation is incomplete: consume nothing
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(sticky, s_err);
+    return;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  LbOpt o = opts[i];
+  if (o.phase == 2) return;
+  const int K = o.K;
+  double* x = o.v;
+  double* g = x + K;
+  double* xp = x + 2 * K;
+  double* gp = x + 3 * K;
+  double* d = x + 4 * K;
+  double* S = x + 5 * K;
+  double* Y = S + kM * K;
+  double* ys_h = Y + kM * K;
+  double* alpha = ys_h + kM;
+
+  o.evals++;
+  const double f = o.loss[0];
+  bool finite = isfinite(f);
+  double wla = 0;
+  for (int k = 0; k < K; ++k) {
+    finite = finite && isfinite(o.dot[k]);
+    wla += o.lam64[k] * o.dot[k];
+  }
+  auto finish = [&](int status, double fret) {
+    o.status = status;
+    o.fret = fret;
+    o.phase = 2;
+  };
+  if (!finite) {  // the kernel domain overflowed at this point
+    finish(WDL_FIT_OVERFLOW, f);
+    opts[i] = o;
+    done[i] = 1;
+    return;
+  }
+  for (int k = 0; k < K; ++k) g[k] = (o.dot[k] - wla) * o.lam64[k];
+
+  // start of a line search from the accepted point x (lbfgs.c:772-790)
+  auto start_ls = [&]() -> bool {
+    for (int k = 0; k < K; ++k) {
+      xp[k] = x[k];
+      gp[k] = g[k];
+    }
+    o.finit = o.f;
+    if (o.step <= 0) {
+      finish(kInvalidParameters, o.f);
+      return false;
+    }
+    o.dginit = dotk(g, d, K);
+    if (o.dginit > 0) {
+      finish(kIncreaseGradient, o.f);
+      return false;
+    }
+    o.count = 0;
+    for (int k = 0; k < K; ++k) x[k] = xp[k] + o.step * d[k];
+    put_weights(o, x);
+    o.phase = 1;
+    return true;
+  };
+
+  if (o.phase == 0) {  // first evaluation (lbfgs.c:423-470)
+    o.f = f;
+    const double xnorm = fmax(sqrt(dotk(x, x, K)), 1.0);
+    const double gnorm = sqrt(dotk(g, g, K));
+    if (gnorm / xnorm <= prm.epsilon) {
+      finish(kAlreadyMinimized, f);
+    } else {
+      for (int k = 0; k < K; ++k) d[k] = -g[k];
+      o.step = 1.0 / sqrt(dotk(d, d, K));
+      o.k = 1;
+      o.end = 0;
+      start_ls();
+    }
+  } else {  // a line-search trial (lbfgs.c:791-867)
+    o.count++;
+    double width = 0;
+    bool accept = false;
+    if (f > o.finit + o.step * prm.ftol * o.dginit) {
+      width = 0.5;
+    } else {
+      const double dg = dotk(g, d, K);
+      if (dg < prm.wolfe * o.dginit) width = 2.1;
+      else if (dg > -prm.wolfe * o.dginit) width = 0.5;
+      else accept = true;
+    }
+    if (!accept) {
+      int fail = 0;
+      if (o.step < prm.min_step) fail = kMinimumStep;
+      else if (o.step > prm.max_step) fail = kMaximumStep;
+      else if (prm.max_linesearch <= o.count) fail = kMaximumLinesearch;
+      if (fail) {  // revert to the previous point (lbfgs.c:487-492)
+        for (int k = 0; k < K; ++k) x[k] = xp[k];
+        finish(fail, o.finit);
+      } else {
+        o.step *= width;
+        for (int k = 0; k < K; ++k) x[k] = xp[k] + o.step * d[k];
+        put_weights(o, x);
+      }
+    } else {  // accepted: convergence tests, then the next direction (lbfgs.c:505-612)
+      o.f = f;
+      const double xnorm = sqrt(dotk(x, x, K));
+      const double gnorm = sqrt(dotk(g, g, K));
+      if (gnorm / fmax(xnorm, 1.0) <= prm.epsilon) {
+        finish(kSuccess, f);
+      } else if (prm.max_iterations != 0 && prm.max_iterations < o.k + 1) {
+        finish(kMaximumIteration, f);
+      } else {
+        double* s_e = S + (size_t)o.end * K;
+        double* y_e = Y + (size_t)o.end * K;
+        for (int k = 0; k < K; ++k) {
+          s_e[k] = x[k] - xp[k];
+          y_e[k] = g[k] - gp[k];
+        }
+        const double ys = dotk(y_e, s_e, K);
+        const double yy = dotk(y_e, y_e, K);
+        ys_h[o.end] = ys;
+        const int bound = o.k < kM ? o.k : kM;
+        o.k++;
+        o.end = (o.end + 1) % kM;
+        for (int k = 0; k < K; ++k) d[k] = -g[k];
+        int j = o.end;
+        for (int b = 0; b < bound; ++b) {
+          j = (j + kM - 1) % kM;
+          alpha[j] = dotk(S + (size_t)j * K, d, K) / ys_h[j];
+          for (int k = 0; k < K; ++k) d[k] -= alpha[j] * Y[(size_t)j * K + k];
+        }
+        for (int k = 0; k < K; ++k) d[k] *= ys / yy;
+        for (int b = 0; b < bound; ++b) {
+          const double beta = dotk(Y + (size_t)j * K, d, K) / ys_h[j];
+          for (int k = 0; k < K; ++k) d[k] += (alpha[j] - beta) * S[(size_t)j * K + k];
+          j = (j + 1) % kM;
+        }
+        o.step = 1.0;
+        start_ls();
+      }
+    }
+  }
+  opts[i] = o;
+  done[i] = o.phase == 2 ? 1 : 0;
+}
+
+struct FitOut {
+  double w[64];
+  double loss;
+  int status, evals;
+};
+
+__global__ void k_fit_outputs(const LbOpt* opts, int n, FitOut* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const LbOpt o = opts[i];
+  const double* x = o.v;
+  double mx = x[0];
+  for (int k = 1; k < o.K; ++k) mx = x[k] > mx ? x[k] : mx;
+  double s = 0;
+  for (int k = 0; k < o.K; ++k) s += exp(x[k] - mx);
+  for (int k = 0; k < o.K; ++k) out[i].w[k] = exp(x[k] - mx) / s;
+  out[i].loss = o.phase == 2 ? o.fret : o.f;
+  out[i].status = o.phase == 2 ? o.status : kMaximumIteration;
+  out[i].evals = o.evals;
+}
+
+inline size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace wdl
+
+using namespace wdl;
+
+extern "C" int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* fp, int nprob, int max_iterations,
+                               double epsilon) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  if (!fp || nprob < 1 || max_iterations < 0 || !(epsilon >= 0))
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "bad arguments");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(ctx, WDL_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = ctx->stream;
+  // The batch layout with weights-only problems; the starting weights are
+  // placeholders that k_fit_init overwrites.
+  std::vector<wdl_problem> pb(nprob);
+  size_t nopt = 0, pool = 0, max_pk = 0;
+  for (int q = 0; q < nprob; ++q) {
+    const wdl_fit_problem& f = fp[q];
+    if (f.K < 1 || f.K > 64 || f.P < 1 || !f.atoms || !f.observed || !f.weights || !f.loss ||
+        !f.status || !f.evaluations)
+      return set_error(ctx, WDL_ERR_INVALID_ARG, "fit problem " + std::to_string(q) + ": bad sizes or pointers");
+    nopt += f.P;
+    pool += (size_t)f.P * pool_doubles(f.K);
+    if ((size_t)f.P * f.K > max_pk) max_pk = (size_t)f.P * f.K;
+  }
+  std::vector<double> ones(max_pk, 1.0);
+  for (int q = 0; q < nprob; ++q) {
+    const wdl_fit_problem& f = fp[q];
+    wdl_problem& w = pb[q];
+    w = wdl_problem{};
+    w.W = f.W;
+    w.H = f.H;
+    w.K = f.K;
+    w.L = f.L;
+    w.P = f.P;
+    w.loss_type = f.loss_type;
+    w.mode = WDL_MODE_WEIGHTS;
+    w.atoms = f.atoms;
+    w.weights = ones.data();
+    w.observed = f.observed;
+  }
+  // extra region: optimiser table, state pool, starting points, outputs, flags
+  const size_t off_opts = 0;
+  const size_t off_pool = a256(off_opts + nopt * sizeof(LbOpt));
+  const size_t off_x0 = a256(off_pool + pool * sizeof(double));
+  const size_t off_out = a256(off_x0 + nopt * 64 * sizeof(double));
+  const size_t off_done = a256(off_out + nopt * sizeof(FitOut));
+  const size_t off_sticky = a256(off_done + nopt);
+  const size_t extra = off_sticky + 256;
+  BatchPlan bp;
+  int rc;
+  if ((rc = batch_prepare(ctx, pb.data(), nprob, extra, bp, s))) return rc;
+  char* ex = bp.base + bp.extra_off;
+  LbOpt* d_opts = reinterpret_cast<LbOpt*>(ex + off_opts);
+  double* d_pool = reinterpret_cast<double*>(ex + off_pool);
+  double* d_x0 = reinterpret_cast<double*>(ex + off_x0);
+  FitOut* d_out = reinterpret_cast<FitOut*>(ex + off_out);
+  uint8_t* d_done = reinterpret_cast<uint8_t*>(ex + off_done);
+  int* d_sticky = reinterpret_cast<int*>(ex + off_sticky);
+
+  std::vector<LbOpt> opts(nopt);
+  std::vector<double> x0(nopt * 64, 0.0);
+  bool any_x0 = false;
+  {
+    size_t i = 0, po = 0;
+    for (int q = 0; q < nprob; ++q) {
+      const wdl_fit_problem& f = fp[q];
+      const BatchBuf& b = bp.buf[q];
+      for (int p = 0; p < f.P; ++p, ++i) {
+        LbOpt o{};
+        o.K = f.K;
+        o.v = d_pool + po;
+        po += pool_doubles(f.K);
+        o.lam64 = b.lam64 + (size_t)p * f.K;
+        o.lam32 = b.lam + (size_t)p * f.K;
+        o.dot = b.dot + (size_t)p * f.K;
+        o.loss = b.loss + p;
+        opts[i] = o;
+        if (f.x0) {
+          any_x0 = true;
+          for (int k = 0; k < f.K; ++k) x0[i * 64 + k] = f.x0[(size_t)p * f.K + k];
+        }
+      }
+    }
+  }
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_opts, opts.data(), nopt * sizeof(LbOpt), cudaMemcpyHostToDevice, s));
+  if (any_x0) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_x0, x0.data(), x0.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(d_done, 0, nopt, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(d_sticky, 0, sizeof(int), s));
+  const unsigned og = (unsigned)((nopt + 127) / 128);
+  k_fit_init<<<og, 128, 0, s>>>(d_opts, (int)nopt, any_x0 ? d_x0 : nullptr);
+  WDL_LAUNCH_CHECK(ctx);
+
+  LbParam prm{max_iterations, 20, epsilon, 1e-4, 0.9, 1e-20, 1e20};
+  // every trial is one round; a histogram needs at most (1 + max_linesearch)
+  // rounds per iteration
+  const long long max_rounds = (long long)(max_iterations > 0 ? max_iterations : 1000) * (prm.max_linesearch + 1) + 2;
+  const int chunk = 4;  // rounds replayed between looks at the done flags
+  std::vector<uint8_t> active(nopt, 1), h_done(nopt, 0);
+  std::vector<int4> items;
+  const bool prof = ctx->profiling;
+  const int trace = ctx->trace_level;
+  ctx->profiling = false;  // no event synchronisation inside a capture
+  ctx->trace_level = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long rounds = 0;
+  int kernels_per_round = 0;
+  auto release = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  };
+  auto restore = [&]() {
+    ctx->profiling = prof;
+    ctx->trace_level = trace;
+  };
+  rc = WDL_OK;
+  while (rounds < max_rounds) {
+    size_t n_active = 0;
+    for (uint8_t a : active) n_active += a;
+    if (!n_active) break;
+    if (!exec) {  // item table of the active histograms, one round captured
+      batch_items(bp, &active, items);
+      cudaError_t e = cudaMemcpyAsync(bp.base + bp.items_off, items.data(), items.size() * sizeof(int4),
+                                      cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) { rc = cuda_error(ctx, e, "item table upload"); break; }
+      const long long l0 = ctx->launches;
+      e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+      if (e != cudaSuccess) { rc = cuda_error(ctx, e, "cudaStreamBeginCapture"); break; }
+      int lr = batch_launch(ctx, bp, items.size(), s);
+      if (!lr) {
+        k_fit_round<<<og, 128, 0, s>>>(d_opts, (int)nopt, prm, bp.sync, d_sticky, d_done);
+        ctx->launches++;
+      }
+      e = cudaStreamEndCapture(s, &graph);
+      if (lr) { rc = lr; break; }
+      if (e != cudaSuccess) { rc = cuda_error(ctx, e, "cudaStreamEndCapture"); break; }
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      if (e != cudaSuccess) { rc = cuda_error(ctx, e, "cudaGraphInstantiate"); break; }
+      kernels_per_round = (int)(ctx->launches - l0);
+      ctx->launches = l0;
+    }
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < chunk && rounds < max_rounds && e == cudaSuccess; ++r, ++rounds) {
+      e = cudaGraphLaunch(exec, s);
+      ctx->launches += kernels_per_round;
+    }
+    int sticky = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_done.data(), d_done, nopt, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sticky, d_sticky, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { rc = cuda_error(ctx, e, "fit round"); break; }
+    if (sticky) { rc = set_error(ctx, sticky, "fused tensor-core kernel: a bounded wait timed out"); break; }
+    bool changed = false;
+    for (size_t i = 0; i < nopt; ++i)
+      if (active[i] && h_done[i]) {
+        active[i] = 0;
+        changed = true;
+      }
+    if (changed) release();
+  }
+  release();
+  restore();
+  if (rc) return rc;
+  k_fit_outputs<<<og, 128, 0, s>>>(d_opts, (int)nopt, d_out);
+  WDL_LAUNCH_CHECK(ctx);
+  std::vector<FitOut> h_out(nopt);
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), d_out, nopt * sizeof(FitOut), cudaMemcpyDeviceToHost, s));
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  size_t i = 0;
+  for (int q = 0; q < nprob; ++q) {
+    const wdl_fit_problem& f = fp[q];
+    for (int p = 0; p < f.P; ++p, ++i) {
+      for (int k = 0; k < f.K; ++k) f.weights[(size_t)p * f.K + k] = h_out[i].w[k];
+      f.loss[p] = h_out[i].loss;
+      f.status[p] = h_out[i].status;
+      f.evaluations[p] = h_out[i].evals;
+    }
+  }
+  return WDL_OK;
+}

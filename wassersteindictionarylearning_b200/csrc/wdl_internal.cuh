@@ -85,6 +85,8 @@ struct wdl_ctx {
   double conv_ms = 0;
   long long conv_launches = 0;
   double conv_images = 0;
+  double log_exps = 0;                 // exps the log-domain passes executed (profiling)
+  unsigned long long* d_taps = nullptr;  // device counter of those exps
   int trace_level = 0;                    // 2: per-phase device trace of the fused kernel
   unsigned long long* d_trace = nullptr;  // [27] accumulated ns / counts
 };
@@ -212,6 +214,35 @@ size_t sk_problem_items(const SkProblem& pr);
 double sk_problem_applications(const SkProblem& pr);
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s);
 int sinkhorn_tc_status(wdl_ctx* ctx, int* sync_dev);
+
+// ---- many problems per launch (batch.cu, fit.cu) ---------------------------------
+struct BatchBuf {  // one problem's device buffers inside the arena
+  double *atoms64, *lam64, *dot, *loss, *obs, *in_atoms, *in_w, *out_la, *out_loss, *out_bary,
+      *out_dic;
+  float *atoms, *lam, *cb, *phi, *acc, *nb, *gwb, *v, *r, *gdic;
+  int* sync;
+};
+struct BatchPlan {
+  int nprob = 0;
+  char* base = nullptr;               // arena base the offsets refer to
+  std::vector<BatchBuf> buf;
+  std::vector<SkProblem> prs;
+  size_t probs = 0, gsync = 0, zero_b = 0, zero_e = 0, in_b = 0, in_e = 0, out_b = 0, out_e = 0;
+  size_t rows_off = 0, outj_off = 0, items_off = 0, extra_off = 0;
+  size_t n_outjobs = 0, n_items_all = 0;
+  int* sync = nullptr;                // work counter, error word of the fused launch
+};
+// Validates, lays out and uploads every problem (inputs normalised on the
+// device); reserves extra_bytes at plan.extra_off for the caller.
+int batch_prepare(wdl_ctx* ctx, const wdl_problem* pb, int nprob, size_t extra_bytes, BatchPlan& bp,
+                  cudaStream_t s);
+// Work items by round (every problem's forward iteration r, then its reverse
+// step 2L-r), for the histograms whose flag in `active` is set (flattened
+// problem by problem; null = all).
+void batch_items(const BatchPlan& bp, const std::vector<uint8_t>* active, std::vector<int4>& items);
+// Clears the accumulated buffers and launches the fused kernel over the first
+// n_items entries of the item table at plan.items_off.
+int batch_launch(wdl_ctx* ctx, BatchPlan& bp, size_t n_items, cudaStream_t s);
 
 // Hot path entry points (sinkhorn.cu); all pointers are device pointers.
 int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
