@@ -238,6 +238,12 @@ int wdl_set_profiling(wdl_ctx* ctx, int level);
 int wdl_phase_trace(wdl_ctx* ctx, double* out27);
 int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launches,
                      double* conv_images);
+/* Launch shapes the autotuner chose on this context: entry i has key {kind,
+ * rows, row length, images, element bytes, signed} (kind 1 = log-domain axis
+ * pass), the chosen variant (rows per block) and its time in ms.
+ * wdl_autotune_count returns the number of entries. */
+int wdl_autotune_count(const wdl_ctx* ctx);
+int wdl_autotune_entry(const wdl_ctx* ctx, int i, long long* key6, int* choice, float* ms);
 /* Exponentials the log-domain operator evaluated while profiling (the
  * reference evaluates one per tap, N*(W+H) per image; taps whose terms are
  * below the sum's rounding are skipped here). */

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 from collections import defaultdict
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -91,7 +92,7 @@ def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6):
 
 
 def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0, max_side=128,
-                epsilon=1e-6):
+                epsilon=1e-6, host_workers=8):
     """problems: dicts with W, H, K, L, gamma, atoms [K*N], observed [N],
     loss_type.  Returns per problem (weights [K], loss, lbfgs status,
     evaluations, domain).
@@ -127,10 +128,18 @@ def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0,
             else:
                 results[i] = (w[0], float(f[0]), int(st[0]), int(ev[0]), "kernel")
     if host:
-        for (i, _, spent), r in zip(host, _fit_host(problems, host, lbfgs_iterations, device,
-                                                    epsilon)):
-            w, f, st, ev, dom = r
-            results[i] = (w, f, st, ev + spent, dom)
+        # host-driven fits in worker threads, each with its own contexts (and
+        # so its own streams): the library calls release the interpreter lock,
+        # so the workers' launches overlap on the GPU
+        workers = max(1, min(host_workers, len(host)))
+        parts = [host[j::workers] for j in range(workers)]
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            outs = list(ex.map(lambda part: _fit_host(problems, part, lbfgs_iterations, device,
+                                                      epsilon), parts))
+        for part, res in zip(parts, outs):
+            for (i, _, spent), r in zip(part, res):
+                w, f, st, ev, dom = r
+                results[i] = (w, f, st, ev + spent, dom)
     return results
 
 

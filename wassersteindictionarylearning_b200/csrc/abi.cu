@@ -2,6 +2,7 @@
 // life cycle, the KernelType operator on host pointers, and the host- and
 // device-pointer forms of the hot path.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -12,6 +13,14 @@
 namespace wdl {
 
 static thread_local std::string g_create_error;
+
+bool autotune_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("WDL_AUTOTUNE");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
 
 int set_error(wdl_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->last_error = msg;
@@ -250,6 +259,8 @@ int wdl_destroy(wdl_ctx* ctx) {
   if (ctx->arena.ptr) cudaFree(ctx->arena.ptr);
   if (ctx->d_trace) cudaFree(ctx->d_trace);
   if (ctx->d_taps) cudaFree(ctx->d_taps);
+  for (auto& gr : ctx->graphs)
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
   if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
   if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -289,6 +300,17 @@ int wdl_phase_trace(wdl_ctx* ctx, double* out27) {
   WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   WDL_CUDA_TRY(ctx, cudaMemcpy(h, ctx->d_trace, sizeof(h), cudaMemcpyDeviceToHost));
   for (int i = 0; i < 27; ++i) out27[i] = (double)h[i];
+  return WDL_OK;
+}
+
+int wdl_autotune_count(const wdl_ctx* ctx) { return ctx ? (int)ctx->tuned.size() : WDL_ERR_INVALID_ARG; }
+
+int wdl_autotune_entry(const wdl_ctx* ctx, int i, long long* key6, int* choice, float* ms) {
+  if (!ctx || i < 0 || i >= (int)ctx->tuned.size()) return WDL_ERR_INVALID_ARG;
+  const auto& e = ctx->tuned[i];
+  if (key6) std::memcpy(key6, e.key, sizeof(e.key));
+  if (choice) *choice = e.choice;
+  if (ms) *ms = e.ms;
   return WDL_OK;
 }
 

@@ -7,6 +7,9 @@
 // image viewed as [R][C] (C contiguous) is contracted along C with the dense
 // C x C factor and written as [C][R], moving the contracted axis to the front.
 // Applying it once per axis returns the image to its original layout.
+#include <cstdlib>
+#include <cstring>
+
 #include "wdl_internal.cuh"
 
 namespace wdl {
@@ -98,19 +101,22 @@ int axis_pass(wdl_ctx* ctx, const T* in, T* out, const T* G, int R, int C, size_
 // the sum goes to out_sign, log|sum| to out (cpp/kernels.h:1123-1136).
 //
 // A block owns LR rows of one image (staged in SMEM with an odd row stride, so
-// the 16 rows a warp reads at one tap fall in 16 different banks) and produces
-// every output of those rows.  Taps are visited outwards from k = c.  With
-// X = max_k in[r][k], every tap at distance >= d has exponent <= -d^2/gamma + X,
-// so:
+// the rows a warp reads at one tap fall in different banks) and produces every
+// output of those rows.  Taps are visited outwards from k = c, both sides per
+// step.  With X = max_k in[r][k], every tap at distance >= d has exponent
+// <= -d^2/gamma + X, so:
 //  * the maximum pass stops at the first d where -d^2/gamma + X <= max so far;
 //  * the sum pass stops at the first d where -d^2/gamma + X < max - kTail; the
-//    taps left out then add at most 2C e^-kTail relative to the largest term,
-//    below the rounding of the sum (kTail = 40 bits for FP32, 60 nats for FP64),
-//    so the result is the full sum's to rounding.
+//    taps left out add at most 2C e^-kTail relative to the largest term, below
+//    the rounding of the sum (kTail = 40 bits for FP32, 60 nats for FP64), so
+//    the result is the full sum's to rounding.
 // FP32 works in base 2 (inputs scaled by log2 e once when staged; ex2 / lg2),
 // FP64 in base e with exp / log.  The summation order (outwards, both sides)
-// differs from the reference's k = 0..C-1; only rounding depends on it.
-constexpr int LR = 16;
+// differs from the reference's k = 0..C-1; only rounding depends on it.  LR
+// (rows per block) is chosen per shape by the autotuner below; every output is
+// computed by the same operations whatever LR is, so the choice never changes
+// a result.
+constexpr int kLogRowsDefault = 16;
 
 template <typename T>
 struct LogOps;
@@ -120,7 +126,13 @@ struct LogOps<float> {
   static constexpr float kUnscale = 0.6931471805599453f;  // ln 2
   static constexpr float kTail = 40.f;                   // bits
   static constexpr float kFloor = -3.402823466e38f;      // start of the maximum
-  __device__ static float ex(float x) { return exp2f(x); }
+  // the hardware base-2 exponential; arguments are <= 0 here and results
+  // below 2^-126 are far under the sum's rounding, so flushing them is exact
+  __device__ static float ex(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  }
   __device__ static float lg(float x) { return log2f(x); }
 };
 template <>
@@ -133,7 +145,7 @@ struct LogOps<double> {
   __device__ static double lg(double x) { return log(x); }
 };
 
-template <typename T, bool SIGNED>
+template <typename T, bool SIGNED, int LR>
 __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
@@ -150,7 +162,7 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
   const size_t base = (size_t)blockIdx.y * img_stride;
   const int nr = min(LR, R - r0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // stage: warp w owns rows w and w + 8, so the row maxima come from shuffles
+  // stage: warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
   for (int rr = warp; rr < LR; rr += 8) {
     T vm = Op::kFloor;
     for (int k = lane; k < C; k += 32) {
@@ -180,30 +192,47 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     if (rr >= nr) continue;
     const T* row = rows + rr * CP;
     const T X = xmax[rr];
-    int dmax = 0;
+    const int dboth = min(c, C - 1 - c);  // both sides inside the row for d <= dboth
+    const int sgnd = c < C - 1 - c ? 1 : -1;  // the side that remains beyond dboth
     T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
-    for (int d = 1; d < C; ++d) {
+    int d = 1;
+    for (; d <= dboth; ++d) {
       const T l = lk[d];
       if (l + X <= m) break;
-      if (c - d >= 0) { const T t = l + row[c - d]; m = t > m ? t : m; }
-      if (c + d < C) { const T t = l + row[c + d]; m = t > m ? t : m; }
+      const T a = l + row[c - d], b = l + row[c + d];
+      const T ab = a > b ? a : b;
+      m = ab > m ? ab : m;
+    }
+    if (d > dboth) {
+      for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
+        const T l = lk[d];
+        if (l + X <= m) break;
+        const T t = l + row[c + sgnd * d];
+        m = t > m ? t : m;
+      }
     }
     const uint8_t* sgn = sg + rr * SP;
     T sum = Op::ex(row[c] - m);
     if (SIGNED && !sgn[c]) sum = -sum;
-    const T floor_ = m - Op::kTail;
-    for (int d = 1; d < C; ++d) {
+    const T fl = m - Op::kTail;
+    int dmax = 0;
+    for (d = 1; d <= dboth; ++d) {
       const T l = lk[d];
-      if (l + X < floor_) break;
+      if (l + X < fl) break;
       dmax = d;
       const T lm = l - m;
-      if (c - d >= 0) {
-        const T ex = Op::ex(lm + row[c - d]);
-        sum += (!SIGNED || sgn[c - d]) ? ex : -ex;
-      }
-      if (c + d < C) {
-        const T ex = Op::ex(lm + row[c + d]);
-        sum += (!SIGNED || sgn[c + d]) ? ex : -ex;
+      const T ea = Op::ex(lm + row[c - d]), eb = Op::ex(lm + row[c + d]);
+      if (SIGNED) sum += (sgn[c - d] ? ea : -ea) + (sgn[c + d] ? eb : -eb);
+      else sum += ea + eb;
+    }
+    if (d > dboth) {
+      for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
+        const T l = lk[d];
+        if (l + X < fl) break;
+        dmax = d;
+        const int k = c + sgnd * d;
+        const T ex = Op::ex((l - m) + row[k]);
+        sum += (!SIGNED || sgn[k]) ? ex : -ex;
       }
     }
     const size_t o = base + (size_t)c * R + (r0 + rr);
@@ -224,9 +253,14 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
 }
 
 template <typename T>
-int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
-                  const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
-  size_t smem = ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
+size_t log_axis_smem(int LR, int C) {
+  return ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
+}
+
+template <typename T, int LR>
+int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
+                    const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+  const size_t smem = log_axis_smem<T>(LR, C);
   const T gamma_t = T(ctx->gamma);
   size_t done = 0;
   while (done < nimg) {
@@ -235,12 +269,12 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
     dim3 grid((R + LR - 1) / LR, (unsigned)chunk);
     size_t off = done * img_stride;
     if (in_sign) {
-      auto k = log_axis_pass_kernel<T, true>;
+      auto k = log_axis_pass_kernel<T, true, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
                                 out_sign + off, ctx->profiling ? ctx->d_taps : nullptr);
     } else {
-      auto k = log_axis_pass_kernel<T, false>;
+      auto k = log_axis_pass_kernel<T, false, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr,
                                 ctx->profiling ? ctx->d_taps : nullptr);
@@ -248,6 +282,64 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
     WDL_LAUNCH_CHECK(ctx);
     done += chunk;
   }
+  return WDL_OK;
+}
+
+
+template <typename T>
+int log_axis_dispatch(wdl_ctx* ctx, int LR, const T* in, T* out, int R, int C, size_t nimg,
+                      size_t img_stride, const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+  switch (LR) {
+    case 8: return log_axis_launch<T, 8>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 32: return log_axis_launch<T, 32>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    default: return log_axis_launch<T, 16>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+  }
+}
+
+// Autotuner: the first call of a shape (rows, row length, image count, type,
+// signed) outside a graph capture runs every candidate rows-per-block on the
+// call's own data, timed with CUDA events on the call's stream, and keeps the
+// fastest for later calls of that shape.  WDL_AUTOTUNE=0 keeps the default.
+template <typename T>
+int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
+                  const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+  const long long key[6] = {1, R, C, (long long)nimg, (long long)sizeof(T), in_sign ? 1 : 0};
+  for (const auto& e : ctx->tuned)
+    if (!std::memcmp(e.key, key, sizeof(key)))
+      return log_axis_dispatch<T>(ctx, e.choice, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  if (!autotune_enabled() || cap != cudaStreamCaptureStatusNone || ctx->profiling)
+    return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+  const int cand[3] = {8, 16, 32};
+  int best = kLogRowsDefault;
+  float best_ms = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WDL_CUDA_TRY(ctx, cudaEventCreate(&e0));
+  WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
+  int rc = WDL_OK;
+  for (int c : cand) {
+    if (log_axis_smem<T>(c, C) > 200 * 1024) continue;
+    cudaEventRecord(e0, s);
+    if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s))) break;
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  wdl_ctx::TuneEntry t;
+  std::memcpy(t.key, key, sizeof(key));
+  t.choice = best;
+  t.ms = best_ms;
+  ctx->tuned.push_back(t);
+  // the candidates computed identical outputs; the last one's stands
   return WDL_OK;
 }
 

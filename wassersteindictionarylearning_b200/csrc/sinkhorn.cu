@@ -14,6 +14,8 @@
 // weight-gradient dot products, the sum of the dictionary gradient over P) runs
 // in FP64.
 #include <cmath>
+#include <cstring>
+#include <functional>
 
 #include "wdl_internal.cuh"
 #include "wdl_math.cuh"
@@ -909,6 +911,59 @@ size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K) {
   return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 16 * 256;
 }
 
+// The CUDA-core path issues ~7 launches per iteration and reverse step (about
+// 800 for L = 60); an L-BFGS loop repeats the same call with the same buffers.
+// The first call with a given key runs eagerly (the workspace settles), the
+// second is captured into a CUDA graph, later ones replay it.  The key holds
+// every size, pointer and the stream, plus the workspace base and size, so a
+// replay touches exactly the memory an eager call would.
+int replay_or_run(wdl_ctx* ctx, const unsigned long long (&key)[20], cudaStream_t s,
+                  const std::function<int()>& run) {
+  if (ctx->profiling || ctx->trace_level || s == nullptr || s == cudaStreamLegacy ||
+      s == cudaStreamPerThread)
+    return run();
+  wdl_ctx::GraphEntry* e = nullptr;
+  for (auto& g : ctx->graphs)
+    if (!std::memcmp(g.key, key, sizeof(key))) e = &g;
+  if (e && e->exec) {
+    ctx->launches += e->launches;
+    WDL_CUDA_TRY(ctx, cudaGraphLaunch(e->exec, s));
+    return WDL_OK;
+  }
+  if (!e) {  // first sighting: eager
+    const int rc = run();
+    if (rc) return rc;
+    if (ctx->graphs.size() >= 8) {
+      if (ctx->graphs.front().exec) cudaGraphExecDestroy(ctx->graphs.front().exec);
+      ctx->graphs.erase(ctx->graphs.begin());
+    }
+    ctx->graphs.emplace_back();
+    std::memcpy(ctx->graphs.back().key, key, sizeof(key));
+    ctx->graphs.back().seen = 1;
+    return WDL_OK;
+  }
+  // second sighting: capture, instantiate, launch
+  const long long l0 = ctx->launches;
+  WDL_CUDA_TRY(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  const int rc = run();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
+  const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    e->exec = nullptr;
+    return cuda_error(ctx, ie, "cudaGraphInstantiate");
+  }
+  e->launches = ctx->launches - l0;
+  WDL_CUDA_TRY(ctx, cudaGraphLaunch(e->exec, s));
+  return WDL_OK;
+}
+
 int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
                       const double* weights, const double* observed, const double* b_init,
                       double* result_la, double* result_dic, double* bary, double* loss,
@@ -916,11 +971,30 @@ int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
   if (use_fused(ctx, loss_type))
     return gradient_both_fused(ctx, P, K, L, loss_type, atoms, weights, observed, b_init, result_la,
                                result_dic, bary, loss, b_last, s, normalise);
-  if (use_fp64(ctx))
-    return gradient_both_t<double>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
-                                   result_la, result_dic, bary, loss, b_last, s, normalise);
-  return gradient_both_t<float>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
-                                result_la, result_dic, bary, loss, b_last, s, normalise);
+  // the workspace is sized before the key is formed, so a replay never needs
+  // a larger one
+  const bool f64 = use_fp64(ctx);
+  const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
+  const size_t need = f64 ? eval_bytes_t<double>(P, K, L, ctx->N, log_domain, loss_type == WDL_LOSS_WASSERSTEIN)
+                          : eval_bytes_t<float>(P, K, L, ctx->N, log_domain, loss_type == WDL_LOSS_WASSERSTEIN);
+  int rc;
+  if ((rc = ensure_arena(ctx, need))) return rc;
+  const unsigned long long key[20] = {
+      1ull, (unsigned long long)P, (unsigned long long)K, (unsigned long long)L,
+      (unsigned long long)loss_type, (unsigned long long)normalise,
+      (unsigned long long)(uintptr_t)atoms, (unsigned long long)(uintptr_t)weights,
+      (unsigned long long)(uintptr_t)observed, (unsigned long long)(uintptr_t)b_init,
+      (unsigned long long)(uintptr_t)result_la, (unsigned long long)(uintptr_t)result_dic,
+      (unsigned long long)(uintptr_t)bary, (unsigned long long)(uintptr_t)loss,
+      (unsigned long long)(uintptr_t)b_last, (unsigned long long)(uintptr_t)s,
+      (unsigned long long)(uintptr_t)ctx->arena.ptr, (unsigned long long)ctx->arena.bytes, 0ull, 0ull};
+  return replay_or_run(ctx, key, s, [&]() {
+    if (f64)
+      return gradient_both_t<double>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
+                                     result_la, result_dic, bary, loss, b_last, s, normalise);
+    return gradient_both_t<float>(ctx, P, K, L, loss_type, atoms, weights, observed, b_init,
+                                  result_la, result_dic, bary, loss, b_last, s, normalise);
+  });
 }
 
 int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,

@@ -89,11 +89,32 @@ struct wdl_ctx {
   unsigned long long* d_taps = nullptr;  // device counter of those exps
   int trace_level = 0;                    // 2: per-phase device trace of the fused kernel
   unsigned long long* d_trace = nullptr;  // [27] accumulated ns / counts
+
+  // Replayable evaluations of the multi-launch (CUDA-core) path: a call whose
+  // sizes, pointers, stream and workspace match a previous call replays that
+  // call's launches as one CUDA graph (sinkhorn.cu).
+  struct GraphEntry {
+    unsigned long long key[20];
+    int seen = 0;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+  };
+  std::vector<GraphEntry> graphs;
+
+  // Autotuned launch shapes (conv_simt.cu): key -> chosen variant.
+  struct TuneEntry {
+    long long key[6];
+    int choice = 0;
+    float ms = 0;
+  };
+  std::vector<TuneEntry> tuned;
 };
 
 namespace wdl {
 
 int set_error(wdl_ctx* ctx, int code, const std::string& msg);
+// WDL_AUTOTUNE=0 in the environment turns the launch-shape autotuner off.
+bool autotune_enabled();
 int cuda_error(wdl_ctx* ctx, cudaError_t e, const char* where);
 int ensure_arena(wdl_ctx* ctx, size_t bytes);
 
