@@ -67,8 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched128",
-                    choices=sorted(WORKLOADS) + ["uneven512", "uneven512-floored"])
+    ap.add_argument("--workload", default="batched128", choices=sorted(WORKLOADS) + ["uneven512"])
     ap.add_argument("--precision", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -258,6 +257,90 @@ def run_ours(args):
     n = x.size
     PK = P * K
     if wl["domain"] == "log":
+        kern = w.CudaLogSignArrayGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
+    else:
+        kern = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=precision, device=local)
+    ctx = kern.ctx
+    L_ = _lib.lib()
+    dev = torch.device("cuda", local)
+    x_d = torch.from_numpy(x).to(dev)
+    obs_d = torch.from_numpy(obs.reshape(-1)).to(dev)
+    g_d = torch.empty(n, dtype=torch.float64, device=dev)
+    f_d = torch.empty(1, dtype=torch.float64, device=dev)
+    # An explicit stream: the library runs on it and the CUDA events below are
+    # recorded on it (handle 0, the legacy default stream, would mean "the
+    # context's own stream" to the C ABI).
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step():
+        rc = L_.wdl_evaluate_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(x_d.data_ptr()),
+                                         C.c_void_p(g_d.data_ptr()), n,
+                                         C.c_void_p(obs_d.data_ptr()), C.c_void_p(f_d.data_ptr()),
+                                         None, None, None, sptr)
+        _lib.check(rc, ctx)
+        if world > 1:  # the path's one exchange: dictionary gradient + loss
+            allreduce_atoms_and_loss(g_d, f_d, PK, dist)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    tape_gb = L_.wdl_eval_bytes(ctx, P, K, L) / 1e9
+
+    launches0 = L_.wdl_launch_count(ctx)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    gpu_launches = L_.wdl_launch_count(ctx) - launches0
+    clocks = clk.summary()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = P * L * args.steps * world
+    value = units / (ms / 1e3)
+    fval = float(f_d.item())
+
+    # Dominant kernel (the separable operator): average duration over one profiled
+    # step, with CUDA events on the launching stream, outside the timed loop.
+    L_.wdl_set_profiling(ctx, 1)
+    step()
+    torch.cuda.synchronize()
+    conv_ms, conv_launches, conv_imgs = C.c_double(), C.c_longlong(), C.c_double()
+    L_.wdl_conv_profile(ctx, C.byref(conv_ms), C.byref(conv_launches), C.byref(conv_imgs))
+    exps = C.c_double()
+    L_.wdl_exp_profile(ctx, C.byref(exps))
+    L_.wdl_set_profiling(ctx, 0)
+    tuned = []
+    key6, choice, tms = (C.c_longlong * 6)(), C.c_int(), C.c_float()
+    for i in range(max(L_.wdl_autotune_count(ctx), 0)):
+        if L_.wdl_autotune_entry(ctx, i, key6, C.byref(choice), C.byref(tms)) == 0:
+            tuned.append(dict(rows=key6[1], row_len=key6[2], images=key6[3], signed=bool(key6[5]),
+                              rows_per_block=choice.value, ms=round(tms.value, 4)))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    flop_per_img = 2.0 * N * (W + H)  # dense separable contraction, both axes
+    products = 3 if precision == "split_bf16" else 1
+    conv_launch_ms = conv_ms.value / max(conv_launches.value, 1)
+    imgs_per_launch = conv_imgs.value / max(conv_launches.value, 1)
+    # algorithmic (useful) FLOPs: one dense contraction per operator application;
+    # the split-BF16 form executes three tensor products for each
+    achieved_tflops = flop_per_img * imgs_per_launch / (conv_launch_ms * 1e-3) / 1e12
+    if wl["domain"] == "log":
         # With the negligible-tail cut the log-sum-exp passes execute a few
         # exps per output (counted on the device), so the operator's floor is
         # HBM: each of the two axis passes reads and writes every image once
@@ -293,8 +376,13 @@ def run_ours(args):
         peak_src = "of nominal CUDA-core FMA peak at max clock"
         bound = "fp32-cuda-core" if precision == "fp32" else "fp64-cuda-core"
     if wl["domain"] != "log":
+        # DRAM bytes of one fused launch at P=64, L=100 from one ncu capture
+        # (profiles/sinkhorn_tc_kernel_batched128_dram.md), scaled by P*L
+        traffic = (28.75e9 * (P * L) / (64 * 100)
+                   if wl["name"] == "batched128" and precision == "split_bf16" else None)
         roofline = dict(bound=bound, achieved=achieved_tflops, peak=peak, unit="TFLOP/s",
-                        frac=achieved_tflops / peak, traffic=None, peak_source=peak_src,
+                        frac=achieved_tflops / peak, traffic=traffic, peak_source=peak_src,
+                        algorithmic_bytes_per_launch=8.0 * K * N * 4 * P * L,
                         executed_tflops=achieved_tflops * products,
                         ceiling_frac=1.0 / products,
                         kernel=(f"fused Sinkhorn kernel: one launch = {imgs_per_launch:.0f} separable-operator "
@@ -397,24 +485,17 @@ def run_uneven(args):
     """The uneven weight-fitting workload: 512 independent problems (side from
     {32,48,64,96,128,192}, K 3-8, L 25-100, gamma {1,2,4}, quadratic loss, 40
     L-BFGS iterations, split-BF16), fitted by batch.fit_weights.  With the
-    workload's peaked random-blob dictionaries the kernel-domain scalings leave
-    the float range within ~10 iterations, so nearly every problem is fitted in
-    the log domain; `--workload uneven512-floored` gives the atoms a uniform
-    floor (half the mass), which keeps the kernel domain in range, so the
-    problems up to 128 run in the device L-BFGS path."""
+    workload's random-blob dictionaries (atoms that differ in where their mass
+    sits) and gamma of 1-4 pixels^2 the kernel-domain scalings leave the float
+    range within ~10 iterations, so every problem ends up fitted in the log
+    domain.  `--P n` fits the first n problems only."""
     import numpy as np
     import torch
 
     from wassersteindictionarylearning_b200.batch import fit_weights, uneven_problems
-    floored = args.workload.endswith("floored")
     n = args.P or 512
     iters = 40
     probs = uneven_problems(n=n, seed=0)
-    if floored:
-        for pr in probs:
-            N = pr["W"] * pr["H"]
-            a = pr["atoms"].reshape(pr["K"], N) + 1.0 / N
-            pr["atoms"] = (a / a.sum(axis=1, keepdims=True)).reshape(-1)
     torch.cuda.set_device(0)
     # warm-up: one small problem per (kind of) path, builds every kernel
     fit_weights(probs[:4], lbfgs_iterations=2)
@@ -434,8 +515,7 @@ def run_uneven(args):
     line = dict(metric="weight fits/s (uneven 512-problem batch)", value=n / el, unit="fits/s",
                 n_gpus=1, steps=1, warmup=1, ms_per_step=el * 1e3, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="bf16x3+f32 (kernel domain), f32 (log domain)",
-                data="synthetic: per problem a seeded random-blob dictionary and one blob histogram"
-                     + (" (atoms with a uniform floor of half their mass)" if floored else ""),
+                data="synthetic: per problem a seeded random-blob dictionary and one blob histogram",
                 config=dict(workload=args.workload, problems=n, sides=[32, 48, 64, 96, 128, 192],
                             K="3-8", L="25-100", gamma=[1, 2, 4], loss="quadratic",
                             lbfgs_iterations=iters, timing="wall clock around the whole fit "
@@ -449,7 +529,7 @@ def run_uneven(args):
 
 def main():
     args = parse()
-    if args.workload.startswith("uneven512"):
+    if args.workload == "uneven512":
         run_uneven(args)
     elif args.impl == "reference":
         run_reference(args)
