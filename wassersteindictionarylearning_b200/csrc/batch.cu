@@ -100,9 +100,10 @@ struct Carve {
 int batch_prepare(wdl_ctx* ctx, const wdl_problem* pb, int nprob, size_t extra_bytes, BatchPlan& bp,
                   cudaStream_t s) {
   if (!ctx || !pb || nprob < 1) return set_error(ctx, WDL_ERR_INVALID_ARG, "bad arguments");
-  if (!ctx->tc || ctx->domain != WDL_DOMAIN_KERNEL)
+  if (!tc_fused(ctx) || ctx->domain != WDL_DOMAIN_KERNEL)
     return set_error(ctx, WDL_ERR_UNSUPPORTED,
-                     "many-problem launches need a kernel-domain WDL_TF32 or WDL_SPLIT_BF16 context");
+                     "many-problem launches need a kernel-domain WDL_TF32 or WDL_SPLIT_BF16 context "
+                     "of a 2-D grid with sides <= 128");
   const bool split = ctx->precision == WDL_SPLIT_BF16;
   for (int q = 0; q < nprob; ++q) {
     const wdl_problem& w = pb[q];

@@ -25,7 +25,8 @@
 namespace wdl {
 
 struct TcResources {
-  int max_side = 128;
+  bool fused = false;    // 2-D with sides <= 128: whole-image operator and fused Sinkhorn kernel
+  uint8_t* factor_blocks[3] = {nullptr, nullptr, nullptr};  // axis-pass operand blocks per axis
   size_t smem_bytes = 0;
   int* d_err = nullptr;  // device status word written on a bounded-wait timeout
 };
@@ -186,30 +187,42 @@ __global__ void __launch_bounds__(256, 1)
 
 }  // namespace
 
+// Tensor-core precisions: every grid with sides up to kTcMaxSide (2-D and 3-D,
+// axis passes of conv_tc_axis.cu); 2-D grids with sides up to one 128-row tile
+// also get the whole-image operator and the fused Sinkhorn kernel.
+constexpr int kTcMaxSide = 512;
+
 bool tc_supported(const wdl_ctx* ctx) {
-  return ctx->ndim == 2 && ctx->W <= tc::kRows && ctx->H <= tc::kRows;
+  return ctx->W <= kTcMaxSide && ctx->H <= kTcMaxSide && ctx->D <= kTcMaxSide;
 }
+
+bool tc_fused(const wdl_ctx* ctx) { return ctx->tc != nullptr && ctx->tc->fused; }
 
 int tc_init(wdl_ctx* ctx) {
   if (!tc_supported(ctx))
-    return set_error(ctx, WDL_ERR_UNSUPPORTED, "tensor-core operator needs a 2-D grid with sides <= 128");
+    return set_error(ctx, WDL_ERR_UNSUPPORTED, "tensor-core operator needs grid sides <= 512");
   auto* r = new TcResources();
+  r->fused = ctx->ndim == 2 && ctx->W <= tc::kRows && ctx->H <= tc::kRows;
   r->smem_bytes = 3 * tc::kTileBytes + 1024 + 64;
   ctx->tc = r;
   WDL_CUDA_TRY(ctx, cudaMalloc(&r->d_err, sizeof(int)));
   WDL_CUDA_TRY(ctx, cudaMemset(r->d_err, 0, sizeof(int)));
-  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_conv2d_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)r->smem_bytes));
-  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_conv2d_kernel<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)r->smem_bytes));
-  return WDL_OK;
+  if (r->fused) {
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_conv2d_kernel<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)r->smem_bytes));
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_conv2d_kernel<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)r->smem_bytes));
+  }
+  return tc_axis_init(ctx, r->factor_blocks);
 }
 
 void tc_free(wdl_ctx* ctx) {
   if (!ctx->tc) return;
   if (ctx->tc->d_err) cudaFree(ctx->tc->d_err);
+  for (auto* b : ctx->tc->factor_blocks)
+    if (b) cudaFree(b);
   delete ctx->tc;
   ctx->tc = nullptr;
 }
@@ -237,7 +250,9 @@ int conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t
   if (ctx->precision == WDL_FP32) return conv_stack_simt_f32(ctx, in, out, tmp, nimg, s);
   if (!ctx->tc) return set_error(ctx, WDL_ERR_UNSUPPORTED, "tensor-core operator not initialised");
   if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
-  int rc = conv_stack_tc(ctx, in, out, nimg, s);
+  int rc = ctx->tc->fused ? conv_stack_tc(ctx, in, out, nimg, s)
+                          : conv_stack_tc_axes(ctx, in, out, tmp, nimg, ctx->tc->factor_blocks,
+                                               ctx->tc->d_err, s);
   if (rc) return rc;
   if (ctx->profiling) {
     cudaEventRecord(ctx->ev_b, s);

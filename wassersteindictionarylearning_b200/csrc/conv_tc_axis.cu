@@ -1,0 +1,300 @@
+// Tensor-core (tcgen05) axis pass for grids whose sides exceed one 128-row
+// tile, and for 3-D grids: the same primitive as the CUDA-core axis pass
+// (conv_simt.cu), an image viewed as [R][C] (C contiguous) contracted along C
+// with the dense C x C Gibbs factor and written as [C][R]:
+//   out[c][r] = sum_k G[c][k] in[r][k]      (cpp/kernels.h:669-699, :762-807)
+// Applying it once per axis returns the image to its layout, as the reference's
+// x-pass into a transposed temporary followed by the y-pass (and z-pass).
+//
+// Each CTA computes a 128 (c) x 128 (r) output tile of one image as a GEMM with
+// M = 128 TMEM lanes = c, N = 128 columns = r, K = C in chunks of 64: A = the
+// factor rows c0.., B = the image rows r0.., both K-major in SMEM (128-byte
+// swizzle), in one of two stages while the tensor cores work on the other.  The
+// factor is prepared once per context as ready-made operand blocks (split into
+// BF16 hi + lo, or rounded to TF32, already in the swizzled layout), so its
+// blocks are plain 16-byte cp.async copies; the image rows are converted from
+// FP32 by the CTA's threads.  The accumulator row of lane c holds
+// out[c][r0..r0+127], so each thread's epilogue stores are 64-byte contiguous
+// runs of one output row.
+//
+// Precision as the 128-tile operator: kind::tf32, or split BF16 with
+// hi*hi + hi*lo + lo*hi accumulated in FP32 (kind::f16).
+#include "tc_common.cuh"
+
+namespace wdl {
+namespace {
+
+using namespace tc;
+
+constexpr int kAxKc = 64;                  // K elements per chunk
+constexpr int kAxTile = 128;               // output tile: 128 c x 128 r
+constexpr size_t kAxOperand = 32 * 1024;   // one 128 x 64 operand (both BF16 planes / TF32)
+constexpr size_t kAxStage = 2 * kAxOperand;  // A + B
+constexpr int kAxThreads = 256;
+
+// 16-byte chunk (8 BF16 hi + 8 lo, or 4 TF32) of row r, elements k0.. of a
+// 128 x 64 operand whose BF16 lo plane starts 16 KB after the hi plane.
+template <bool SPLIT>
+__device__ __forceinline__ void put_axis_chunk(uint8_t* tile, int r, int k0, const float* v) {
+  if (SPLIT) {
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+      const float2 hf = __bfloat1622float2(h);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
+      hi[q] = *reinterpret_cast<const uint32_t*>(&h);
+      lo[q] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+    const uint32_t o = swz(r, k0, 2);
+    *reinterpret_cast<uint4*>(tile + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(tile + kRegionBytes + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  } else {
+    *reinterpret_cast<uint4*>(tile + swz(r, k0, 4)) =
+        make_uint4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+  }
+}
+
+// Rows row0.. (at most `rows` valid) of a row-major matrix with `len` elements
+// per row, elements kb..kb+63 (zero beyond len), into a 128 x 64 operand.
+template <bool SPLIT>
+__device__ __forceinline__ void stage_operand(uint8_t* tile, const float* __restrict__ src, int rows,
+                                              int len, int kb, bool vec, int t) {
+  constexpr int CE = SPLIT ? 8 : 4;
+  constexpr int CPR = kAxKc / CE;            // chunks per row
+  constexpr int PER = kAxTile * CPR / kAxThreads;  // chunks per thread
+  float v[PER][CE];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int c = t + u * kAxThreads;
+    const int r = c / CPR, k0 = kb + (c - r * CPR) * CE;
+    const float* row = src + (size_t)r * len;
+    if (r < rows && vec && k0 + CE <= len) {
+#pragma unroll
+      for (int q = 0; q < CE; q += 4) {
+        const float4 f = __ldg(reinterpret_cast<const float4*>(row + k0 + q));
+        v[u][q] = f.x; v[u][q + 1] = f.y; v[u][q + 2] = f.z; v[u][q + 3] = f.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < CE; ++q) v[u][q] = (r < rows && k0 + q < len) ? __ldg(row + k0 + q) : 0.f;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int c = t + u * kAxThreads;
+    const int r = c / CPR, kk = (c - r * CPR) * CE;
+    put_axis_chunk<SPLIT>(tile, r, kk, v[u]);
+  }
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The factor of one axis (C x C) as operand blocks: block (m, j) holds rows
+// 128m.. and K elements 64j.. in the SMEM layout of a 128 x 64 operand.
+template <bool SPLIT>
+__global__ void k_build_factor_blocks(const float* __restrict__ G, int C, uint8_t* __restrict__ blocks) {
+  const int nch = (C + kAxKc - 1) / kAxKc;
+  const int m = blockIdx.x / nch, j = blockIdx.x - m * nch;
+  uint8_t* tile = blocks + (size_t)blockIdx.x * kAxOperand;
+  const int c0 = m * kAxTile;
+  constexpr int CE = SPLIT ? 8 : 4;
+  constexpr int CPR = kAxKc / CE;
+  for (int c = threadIdx.x; c < kAxTile * CPR; c += blockDim.x) {
+    const int r = c / CPR, kk = (c - r * CPR) * CE;
+    float v[CE];
+    for (int q = 0; q < CE; ++q) {
+      const int row = c0 + r, k = j * kAxKc + kk + q;
+      v[q] = (row < C && k < C) ? G[(size_t)row * C + k] : 0.f;
+    }
+    put_axis_chunk<SPLIT>(tile, r, kk, v);
+  }
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(kAxThreads, 1)
+    tc_axis_kernel(const float* __restrict__ in, float* __restrict__ out,
+                   const uint8_t* __restrict__ gblocks, int R, int C, size_t img_stride, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 2 * kAxStage);  // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + 2 * kAxStage + 16);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int c0 = blockIdx.x * kAxTile, r0 = blockIdx.y * kAxTile;
+  const float* src = in + (size_t)blockIdx.z * img_stride + (size_t)r0 * C;
+  const int nch = (C + kAxKc - 1) / kAxKc;
+  const uint8_t* gsrc = gblocks + (size_t)blockIdx.x * nch * kAxOperand;
+  float* dst = out + (size_t)blockIdx.z * img_stride;
+  const int b_rows = min(kAxTile, R - r0);
+  const bool vec = (C & 3) == 0;
+
+  if (t == 0) {
+    ptx::mbar_init(ptx::smem_addr(&bars[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[1]), 1);
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tslot), 128);
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t d = *tslot;
+
+  using F = Fmt<SPLIT>;
+  const uint32_t id = ptx::idesc(F::fmt, 128, 128);
+  bool ok = true;
+  for (int j = 0; j < nch; ++j) {
+    const int st = j & 1;
+    uint8_t* a_tile = base + st * kAxStage;
+    uint8_t* b_tile = a_tile + kAxOperand;
+    if (j >= 2) {  // the MMAs of chunk j-2 read this stage: wait for their commit
+      const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[st]), (uint32_t)(((j - 2) >> 1) & 1), kWaitNs);
+      ok = __syncthreads_and(w) != 0;
+      if (!ok) break;
+    }
+    {  // factor block: 32 KB, 8 x 16 bytes per thread, straight copies
+      const uint8_t* gb = gsrc + (size_t)j * kAxOperand;
+      const uint32_t a_s = ptx::smem_addr(a_tile);
+#pragma unroll
+      for (int u = 0; u < (int)(kAxOperand / 16 / kAxThreads); ++u) {
+        const int o = (t + u * kAxThreads) * 16;
+        cp_async16(a_s + o, gb + o);
+      }
+      cp_async_commit();
+    }
+    stage_operand<SPLIT>(b_tile, src, b_rows, C, j * kAxKc, vec, t);
+    cp_async_wait_all();
+    ptx::fence_proxy_async_smem();
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      ptx::tc_fence_after();
+      const uint32_t a = ptx::smem_addr(a_tile), b = ptx::smem_addr(b_tile);
+      const int steps = kAxKc / F::kstep;
+#pragma unroll
+      for (int ks = 0; ks < steps; ++ks) {
+        const uint32_t byte = (uint32_t)ks * 32u;
+        const uint32_t off = (byte >> 7) * kRegionBytes + (byte & 127u);
+        const uint32_t acc = (j > 0 || ks > 0) ? 1u : 0u;
+        const uint64_t ad = ptx::sw128_desc(a + off), bd = ptx::sw128_desc(b + off);
+        if (SPLIT) {
+          const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + off);
+          const uint64_t blo = ptx::sw128_desc(b + kRegionBytes + off);
+          ptx::mma_bf16(d, ad, bd, id, acc);
+          ptx::mma_bf16(d, ad, blo, id, 1u);
+          ptx::mma_bf16(d, alo, bd, id, 1u);
+        } else {
+          ptx::mma_tf32(d, ad, bd, id, acc);
+        }
+      }
+      ptx::mma_commit(ptx::smem_addr(&bars[st]));
+    }
+  }
+  if (ok) {  // the last commit covers every MMA issued before it
+    const int j = nch - 1;
+    const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[j & 1]), (uint32_t)((j >> 1) & 1), kWaitNs);
+    ok = __syncthreads_and(w) != 0;
+  }
+  if (!ok) {
+    if (t == 0) atomicExch(err, WDL_ERR_TIMEOUT);
+  } else {
+    ptx::tc_fence_after();
+    const int q = warp & 3, half = warp >> 2;
+    const int c = c0 + q * 32 + lane;
+    const bool rvec = (R & 3) == 0;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+      float v[16];
+      const int col = half * 64 + cc * 16;
+      ptx::tmem_ld16(d + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
+      ptx::tmem_ld_wait();
+      if (c < C) {
+        float* orow = dst + (size_t)c * R;
+        const int rb = r0 + col;
+#pragma unroll
+        for (int i = 0; i < 16; i += 4) {
+          const int r = rb + i;
+          if (rvec && r + 3 < R) {
+            *reinterpret_cast<float4*>(orow + r) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          } else {
+            for (int e = 0; e < 4; ++e)
+              if (r + e < R) orow[r + e] = v[i + e];
+          }
+        }
+      }
+    }
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  if (warp == 0) ptx::tmem_dealloc(d, 128);
+}
+
+size_t axis_smem() { return 2 * kAxStage + 1024 + 64; }
+
+int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
+                 size_t img_stride, int* err, cudaStream_t s) {
+  size_t done = 0;
+  while (done < nimg) {
+    size_t chunk = nimg - done;
+    if (chunk > 65535) chunk = 65535;
+    dim3 grid((C + kAxTile - 1) / kAxTile, (R + kAxTile - 1) / kAxTile, (unsigned)chunk);
+    if (ctx->precision == WDL_SPLIT_BF16)
+      tc_axis_kernel<true><<<grid, kAxThreads, axis_smem(), s>>>(in + done * img_stride, out + done * img_stride,
+                                                                 G, R, C, img_stride, err);
+    else
+      tc_axis_kernel<false><<<grid, kAxThreads, axis_smem(), s>>>(in + done * img_stride, out + done * img_stride,
+                                                                  G, R, C, img_stride, err);
+    WDL_LAUNCH_CHECK(ctx);
+    done += chunk;
+  }
+  return WDL_OK;
+}
+
+}  // namespace
+
+size_t factor_block_bytes(int C) {
+  const size_t nm = (C + kAxTile - 1) / kAxTile, nch = (C + kAxKc - 1) / kAxKc;
+  return nm * nch * kAxOperand;
+}
+
+// Sets the kernels' SMEM limit and builds the factor blocks of every axis
+// (blocks[a], at most 4 x 8 x 32 KB = 1 MB per axis for sides up to 512).
+int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]) {
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)axis_smem()));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)axis_smem()));
+  const bool split = ctx->precision == WDL_SPLIT_BF16;
+  for (int a = 0; a < ctx->ndim; ++a) {
+    const int C = ctx->axis_len[a];
+    WDL_CUDA_TRY(ctx, cudaMalloc(&blocks[a], factor_block_bytes(C)));
+    const unsigned nb = (unsigned)(factor_block_bytes(C) / kAxOperand);
+    if (split) k_build_factor_blocks<true><<<nb, 256>>>(ctx->G32[a], C, blocks[a]);
+    else k_build_factor_blocks<false><<<nb, 256>>>(ctx->G32[a], C, blocks[a]);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  WDL_CUDA_TRY(ctx, cudaDeviceSynchronize());
+  return WDL_OK;
+}
+
+// The operator as axis passes, as the CUDA-core form: 2-D x then y through
+// tmp; 3-D x, y, z.
+int conv_stack_tc_axes(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                       uint8_t* const (&blocks)[3], int* err, cudaStream_t s) {
+  const int W = ctx->W, H = ctx->H, D = ctx->D;
+  const size_t N = ctx->N;
+  int rc;
+  if (ctx->ndim == 2) {
+    if ((rc = tc_axis_pass(ctx, in, tmp, blocks[0], H, W, nimg, N, err, s))) return rc;
+    return tc_axis_pass(ctx, tmp, out, blocks[1], W, H, nimg, N, err, s);
+  }
+  if ((rc = tc_axis_pass(ctx, in, out, blocks[0], D * H, W, nimg, N, err, s))) return rc;
+  if ((rc = tc_axis_pass(ctx, out, tmp, blocks[1], W * D, H, nimg, N, err, s))) return rc;
+  return tc_axis_pass(ctx, tmp, out, blocks[2], H * W, D, nimg, N, err, s);
+}
+
+}  // namespace wdl

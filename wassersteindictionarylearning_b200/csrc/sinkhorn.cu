@@ -244,21 +244,38 @@ __global__ void k_wloss(const T* __restrict__ v1, const double* __restrict__ v2,
   if (threadIdx.x == 0) loss[p] = gamma * acc;
 }
 
+// The reverse passes' per-(p, k) dot products are summed in two levels with a
+// fixed order: blocks over kSegElems-element segments of each image write
+// partial sums, k_add_partials adds them segment by segment.  The segments
+// depend only on N, so a histogram's result does not depend on P or K.
+constexpr size_t kSegElems = 2048;
+inline size_t n_segments(size_t N) { return (N + kSegElems - 1) / kSegElems; }
+
+__global__ void k_add_partials(double* __restrict__ dot, const double* __restrict__ part, int PK,
+                               int nseg) {
+  const int pk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pk >= PK) return;
+  double s = 0;
+  for (int g = 0; g < nseg; ++g) s += part[(size_t)pk * nseg + g];
+  dot[pk] += s;
+}
+
 // ---------------- kernel-domain reverse pass (:602-673), one round s ----------------
-// Block per (p, k): dictionary tmp = (lambda n - v) * b[s]; weights
+// Block per ((p, k), segment): dictionary tmp = (lambda n - v) * b[s]; weights
 // dot += sum_j log(phi[s]) gw (plain log, as :649), u = (lambda gw - r) / phi[s].
 template <typename T>
 __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
                           const T* __restrict__ b_s, const T* __restrict__ gw,
                           const T* __restrict__ r, const T* __restrict__ phi_s,
                           const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u,
-                          double* __restrict__ dot, int K, size_t N) {
+                          double* __restrict__ part, int K, size_t N) {
   __shared__ double sh[32];
   const size_t pk = blockIdx.x, p = pk / K;
   const T l = lam[pk];
   const size_t base = pk * N, pb = p * N;
+  const size_t j0 = (size_t)blockIdx.y * kSegElems, j1 = min(N, j0 + kSegElems);
   double acc = 0;
-  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+  for (size_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
     const size_t i = base + j;
     tmp[i] = (l * n[pb + j] - v[i]) * b_s[i];
     const T ph = phi_s[i];
@@ -267,7 +284,7 @@ __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
     u[i] = (l * g - r[i]) / ph;
   }
   acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) dot[pk] += acc;
+  if (threadIdx.x == 0) part[pk * gridDim.y + blockIdx.y] = acc;
 }
 
 // gradDic += c / cb[s-1]; tmp = -p c / cb^2; convu *= -p / cb^2 (:612-617, :655-660).
@@ -316,13 +333,14 @@ __global__ void k_lbwd_pre(const T* __restrict__ n, const T* __restrict__ v,
                            const T* __restrict__ r, const T* __restrict__ phi_s,
                            const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u,
                            uint8_t* __restrict__ sd, uint8_t* __restrict__ sw,
-                           double* __restrict__ dot, int K, size_t N) {
+                           double* __restrict__ part, int K, size_t N) {
   __shared__ double sh[32];
   const size_t pk = blockIdx.x, p = pk / K;
   const T l = lam[pk];
   const size_t base = pk * N, pb = p * N;
+  const size_t j0 = (size_t)blockIdx.y * kSegElems, j1 = min(N, j0 + kSegElems);
   double acc = 0;
-  for (size_t j = threadIdx.x; j < N; j += blockDim.x) {
+  for (size_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
     const size_t i = base + j;
     const T x = l * n[pb + j] + v[i];
     sd[i] = x >= T(0);
@@ -335,7 +353,7 @@ __global__ void k_lbwd_pre(const T* __restrict__ n, const T* __restrict__ v,
     u[i] = d_log<T>(fabs(y)) - ph;
   }
   acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) dot[pk] += acc;
+  if (threadIdx.x == 0) part[pk * gridDim.y + blockIdx.y] = acc;
 }
 
 template <typename T>
@@ -457,7 +475,7 @@ template <typename T>
 struct EvalBufs {
   T *atoms, *lam, *tape_b, *tape_cb, *tape_phi, *a, *bary, *n, *gw, *buf2, *cbuf2, *v, *r, *ctmp;
   T *wa = nullptr, *wb = nullptr, *wc = nullptr, *wgrad = nullptr;
-  double *atoms64, *lam64, *gdic, *dot, *loss;
+  double *atoms64, *lam64, *gdic, *dot, *loss, *dpart;
   uint8_t *sd = nullptr, *sw = nullptr, *stmp = nullptr;
 
   template <class A>
@@ -483,6 +501,7 @@ struct EvalBufs {
     d(lam64, P * K);
     d(gdic, PKN);
     d(dot, P * K);
+    d(dpart, P * K * n_segments(N));
     d(loss, P);
     if (wloss) {
       t(wa, PN);
@@ -619,7 +638,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
     const bool more = sstep > 1;
     const size_t nimg = (size_t)(more ? 2 : 1) * P * K;
     if (!log_domain) {
-      k_bwd_pre<T><<<P * K, 256, 0, s>>>(B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dot, K, N);
+      k_bwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
+          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dpart, K, N);
+      WDL_LAUNCH_CHECK(ctx);
+      k_add_partials<<<(P * K + 127) / 128, 128, 0, s>>>(B.dot, B.dpart, P * K, (int)n_segments(N));
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
       k_bwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, PKN, more);
@@ -631,8 +653,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN);
       WDL_LAUNCH_CHECK(ctx);
     } else {
-      k_lbwd_pre<T><<<P * K, 256, 0, s>>>(B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.sd,
-                                          B.sw, B.dot, K, N);
+      k_lbwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
+          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.sd, B.sw, B.dpart, K, N);
+      WDL_LAUNCH_CHECK(ctx);
+      k_add_partials<<<(P * K + 127) / 128, 128, 0, s>>>(B.dot, B.dpart, P * K, (int)n_segments(N));
       WDL_LAUNCH_CHECK(ctx);
       // sd and sw are adjacent, so the pair is one 2*P*K-image signed operand.
       if ((rc = log_conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, B.sd, B.sd, B.stmp, s)))
@@ -769,7 +793,7 @@ size_t fused_bytes(size_t P, size_t K, size_t L, size_t N, bool b_init, bool fwd
 }
 
 bool use_fused(const wdl_ctx* ctx, int loss_type) {
-  return ctx->tc != nullptr && ctx->domain == WDL_DOMAIN_KERNEL && loss_type != WDL_LOSS_WASSERSTEIN;
+  return tc_fused(ctx) && ctx->domain == WDL_DOMAIN_KERNEL && loss_type != WDL_LOSS_WASSERSTEIN;
 }
 
 int prepare_fused(wdl_ctx* ctx, FusedBufs& B, int P, int K, const double* atoms,
@@ -895,7 +919,7 @@ bool use_fp64(const wdl_ctx* ctx) { return ctx->precision == WDL_FP64; }
 
 size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L) {
   const bool log_domain = ctx->domain == WDL_DOMAIN_LOG;
-  if (ctx->tc && !log_domain) {
+  if (tc_fused(ctx) && !log_domain) {
     const size_t a = fused_bytes(P, K, L, ctx->N, true, false);
     const size_t b = eval_bytes_t<float>(P, K, L, ctx->N, false, true);  // Wasserstein loss runs unfused
     return a > b ? a : b;
@@ -905,7 +929,7 @@ size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L) {
 }
 
 size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K) {
-  if (ctx->tc && ctx->domain == WDL_DOMAIN_KERNEL) return fused_bytes(P, K, 2, ctx->N, false, true);
+  if (tc_fused(ctx) && ctx->domain == WDL_DOMAIN_KERNEL) return fused_bytes(P, K, 2, ctx->N, false, true);
   const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
   const size_t t = use_fp64(ctx) ? 8 : 4;
   return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 16 * 256;

@@ -194,6 +194,12 @@ void tc_free(wdl_ctx* ctx);
 // wait gives up (WDL_ERR_TIMEOUT); WDL_OK otherwise.
 int tc_check_status(wdl_ctx* ctx);
 bool tc_supported(const wdl_ctx* ctx);
+// The context has the fused Sinkhorn kernel (tensor-core precision, 2-D, sides <= 128).
+bool tc_fused(const wdl_ctx* ctx);
+// Tensor-core axis passes (conv_tc_axis.cu): any tensor-core context.
+int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]);
+int conv_stack_tc_axes(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
+                       uint8_t* const (&blocks)[3], int* err, cudaStream_t s);
 
 // Fused persistent tensor-core Sinkhorn kernel (sinkhorn_tc.cu).
 // One problem of a fused launch: P histograms on one W x H grid (sides <= 128)
