@@ -273,11 +273,11 @@ int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]) {
     const int C = ctx->axis_len[a];
     WDL_CUDA_TRY(ctx, cudaMalloc(&blocks[a], factor_block_bytes(C)));
     const unsigned nb = (unsigned)(factor_block_bytes(C) / kAxOperand);
-    if (split) k_build_factor_blocks<true><<<nb, 256>>>(ctx->G32[a], C, blocks[a]);
-    else k_build_factor_blocks<false><<<nb, 256>>>(ctx->G32[a], C, blocks[a]);
+    if (split) k_build_factor_blocks<true><<<nb, 256, 0, ctx->stream>>>(ctx->G32[a], C, blocks[a]);
+    else k_build_factor_blocks<false><<<nb, 256, 0, ctx->stream>>>(ctx->G32[a], C, blocks[a]);
     WDL_LAUNCH_CHECK(ctx);
   }
-  WDL_CUDA_TRY(ctx, cudaDeviceSynchronize());
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return WDL_OK;
 }
 
