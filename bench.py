@@ -18,7 +18,9 @@ across ranks with one NCCL all-reduce per step (the path's only exchange).
 The headline line is the batched 128x128 workload.  `--workload dict64`
 (64x64, K=4, L=25, gamma=2, quadratic, FP32 kernel domain) and `--workload
 log256` (256x256, K=8, L=200, gamma=0.5, TV, FP32 log domain) measure the
-other two dictionary-learning configurations the same way.
+other two dictionary-learning configurations the same way; `--workload
+images272` measures the grid of the reference's bundled images (272x240, K=4,
+L=50, split-BF16 through the tensor-core axis passes).
 """
 from __future__ import annotations
 
@@ -47,6 +49,10 @@ WORKLOADS = {
     "log256": dict(name="log256", P=32, W=256, H=256, K=8, L=200, gamma=0.5, loss=1,
                    loss_name="TV", n_blobs=(1, 3), std_frac=(0.01, 0.04), domain="log",
                    precision="fp32", cpu_P=1, cpu_L=4),
+    # the grid of the reference's bundled heart images (272 x 240), synthetic data
+    "images272": dict(name="images272", P=8, W=272, H=240, K=4, L=50, gamma=25.0, loss=2,
+                      loss_name="quadratic", n_blobs=(1, 3), std_frac=(0.03, 0.12),
+                      domain="kernel", precision=None, cpu_P=1, cpu_L=10),
 }
 
 
