@@ -525,7 +525,8 @@ def run_uneven(args):
                 config=dict(workload=args.workload, problems=n, sides=[32, 48, 64, 96, 128, 192],
                             K="3-8", L="25-100", gamma=[1, 2, 4], loss="quadratic",
                             lbfgs_iterations=iters, timing="wall clock around the whole fit "
-                            "(host-driven log-domain fits run in 8 threads on their own streams)"),
+                            "(kernel-domain device fits per gamma, then one persistent log-domain "
+                            "launch per gamma)"),
                 hist_iter_per_s=hist_iters / el,
                 evaluations=dict(total=int(evals.sum()), mean=float(evals.mean())),
                 domains=dict(kernel=doms.count("kernel"), log=doms.count("log")),

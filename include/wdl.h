@@ -192,6 +192,19 @@ typedef struct {
 } wdl_fit_problem;
 int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* problems, int nproblems, int max_iterations,
                     double epsilon);
+/* The same fit in the LOG domain (compute_gradient_both_log_signArray,
+ * cpp/inverseWasserstein.h:678-814, restricted to the forward pass, the loss
+ * and the weight recursion), for problems whose kernel-domain scalings leave
+ * the float range: ONE persistent launch in which every histogram's whole
+ * L-BFGS fit runs on the device (one CTA per histogram up to sides of 32, a
+ * cluster of 2, 4 or 8 CTAs up to 64, 128, 512).  Context: 2-D,
+ * WDL_DOMAIN_LOG, FP32 arithmetic;
+ * its gamma serves every problem.  Sides <= 512, K <= 16, loss 1, 2 or 4.
+ * status[p] is liblbfgs' return code, or WDL_ERR_NONFINITE if an evaluation
+ * was not finite.  No reference counterpart beyond regress_both run one
+ * problem at a time. */
+int wdl_fit_weights_log(wdl_ctx* ctx, const wdl_fit_problem* problems, int nproblems, int max_iterations,
+                        double epsilon);
 
 /* ---- Device-resident forms (device pointers, stream as void*) ----------------
  * Same semantics as the host forms; no host<->device copies, no synchronisation.

@@ -164,3 +164,28 @@ def test_device_lbfgs_reports_overflow():
     (w, f, st, ev), = fit_device(kern, [pr], lbfgs_iterations=5)
     kern.close()
     assert st[0] == WDL_FIT_OVERFLOW and ev[0] == 1
+
+
+def test_persistent_log_fit_matches_host_log_fit(oracle):
+    """wdl_fit_weights_log (every fit wholly on the device, one launch; a
+    cluster of 8 CTAs for the side above 128) against the host L-BFGS driving
+    the log-domain operator path on the same problems."""
+    from wassersteindictionarylearning_b200 import CudaLogSignArrayGaussian2DKernel
+    from wassersteindictionarylearning_b200.batch import _fit_host, fit_device, uneven_problems
+    probs = [p for p in uneven_problems(n=16, seed=5, sides=(24, 40, 144), K_range=(3, 5),
+                                        L_range=(6, 12), gammas=(2.0,))]
+    kern = CudaLogSignArrayGaussian2DKernel(2.0, 512, 512, precision="fp32")
+    outs = fit_device(kern, probs, lbfgs_iterations=8, epsilon=1e-6, log_domain=True)
+    kern.close()
+    host = _fit_host(probs, [(i, "log", 0) for i in range(len(probs))], 8, 0, 1e-6)
+    assert any(p["W"] > 128 for p in probs) and any(p["W"] <= 128 for p in probs)
+    for pr, (w, f, st, ev), (wh, fh, sth, evh, dom) in zip(probs, outs, host):
+        assert dom == "log" and st[0] in (0, -997, -998, 2) and ev[0] >= 2
+        assert abs(w[0].sum() - 1) < 1e-12
+        assert abs(f[0] - fh) <= 1e-3 * abs(fh)
+        assert np.max(np.abs(w[0] - wh)) < 2e-2
+        # the reported loss is the FP64 oracle's at the returned weights
+        W, H, K, L = pr["W"], pr["H"], pr["K"], pr["L"]
+        bary = oracle.barycenter(W, H, 1, 2.0, K, L, pr["atoms"].reshape(K, -1), w[0])
+        f_ref, _ = oracle.loss(2, W, H, 1, 2.0, bary, pr["observed"])
+        assert abs(f[0] - f_ref) <= 1e-3 * abs(f_ref)

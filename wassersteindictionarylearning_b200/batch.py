@@ -12,9 +12,11 @@ histograms of all problems in ONE launch and advances every optimisation in
 a second kernel, the round replayed as a CUDA graph.
 
 `fit_weights` is the uneven-workload driver around it: problems of sides up to
-128 go to the device per gamma; problems above the tile, and problems whose
-kernel-domain scalings overflow, are fitted with the host L-BFGS on the FP32
-operator path of their own grid, in the log domain where needed.
+128 go to the kernel-domain device fit per gamma; problems above the tile, and
+problems whose kernel-domain scalings overflow, go to the log-domain fit
+(wdl_fit_weights_log: one persistent launch per gamma, every fit wholly on the
+device).  `_fit_host` keeps the host-driven form (host L-BFGS around the
+operator path), the reference's control flow, for comparison.
 """
 from __future__ import annotations
 
@@ -63,12 +65,13 @@ def batch_run(kernel, problems):
     return outs
 
 
-def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6):
+def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6, log_domain=False):
     """wdl_fit_weights: every histogram of every problem fitted by its own
     L-BFGS on the device, all evaluated together each round.  problems: dicts
     with W, H, K, L, atoms [K*N], observed [P*N] (P = len / N), loss_type,
     optional x0 [P*K].  Returns per problem (weights [P,K], loss [P], status
-    [P], evaluations [P])."""
+    [P], evaluations [P]).  log_domain: wdl_fit_weights_log on a log-domain
+    kernel (one persistent launch, each fit wholly on the device)."""
     n = len(problems)
     arr = (WdlFitProblem * n)()
     keep, outs = [], []
@@ -86,36 +89,36 @@ def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6):
         arr[i] = WdlFitProblem(W, H, K, L, P, int(pr.get("loss_type", 2)), dptr(atoms), dptr(obs),
                                dptr(x0), dptr(w), dptr(f), st.ctypes.data_as(C.POINTER(C.c_int)),
                                ev.ctypes.data_as(C.POINTER(C.c_int)))
-    check(lib().wdl_fit_weights(kernel.ctx, C.cast(arr, C.c_void_p), n, int(lbfgs_iterations),
-                                float(epsilon)), kernel.ctx)
+    fn = lib().wdl_fit_weights_log if log_domain else lib().wdl_fit_weights
+    check(fn(kernel.ctx, C.cast(arr, C.c_void_p), n, int(lbfgs_iterations), float(epsilon)), kernel.ctx)
     return [(w.reshape(P, K), f, st, ev) for (w, f, st, ev, P, K) in outs]
 
 
 def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0, max_side=128,
-                epsilon=1e-6, host_workers=8):
+                epsilon=1e-6):
     """problems: dicts with W, H, K, L, gamma, atoms [K*N], observed [N],
     loss_type.  Returns per problem (weights [K], loss, lbfgs status,
     evaluations, domain).
 
-    Problems whose side fits the tensor-core tile are fitted on the device,
-    all problems of a gamma in one wdl_fit_weights call (L-BFGS on the device,
-    one fused launch per round).  The kernel domain's scalings grow with the
-    iterations wherever the atoms are nearly empty (the dual potentials reach
-    |d|^2 / gamma, far beyond any float range for peaked atoms, a narrow kernel
-    and long runs); a problem whose kernel-domain evaluation comes back
-    non-finite is fitted again from its start in the log domain (the
-    reference's LogSignArray kernels, cpp/kernels.h:1034), with the host
-    L-BFGS (lbfgs.lbfgs_steps, liblbfgs' parameters) batched by rounds.
-    Problems with a side above the tile run on the FP32 operator path of their
-    own grid with the same escalation."""
+    Problems whose side fits the tensor-core tile are fitted in the kernel
+    domain on the device, all problems of a gamma in one wdl_fit_weights call
+    (L-BFGS on the device, one fused launch per round).  The kernel domain's
+    scalings grow with the iterations when the atoms put their mass in
+    different places (they tend to exp(d^2 / gamma) for transport distances
+    d, far beyond any float range for a narrow kernel and long runs); a problem
+    whose kernel-domain evaluation comes back non-finite is fitted again from
+    its start in the log domain (the reference's LogSignArray kernels,
+    cpp/kernels.h:1034).  Problems with a side above the tile go to the log
+    domain directly.  The log-domain fits of a gamma run as ONE persistent
+    launch (wdl_fit_weights_log), every fit wholly on the device."""
     results = [None] * len(problems)
-    host = []      # (index, starting domain, evaluations already spent)
+    logq = defaultdict(list)      # gamma -> [(index, evaluations already spent)]
     by_gamma = defaultdict(list)
     for i, pr in enumerate(problems):
         if max(pr["W"], pr["H"]) <= max_side:
             by_gamma[pr["gamma"]].append(i)
         else:
-            host.append((i, "kernel", 0))
+            logq[pr["gamma"]].append((i, 0))
     for g, idx in by_gamma.items():
         kern = CudaGaussian2DKernel(g, max_side, max_side, precision=precision, device=device)
         try:
@@ -124,22 +127,27 @@ def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0,
             kern.close()
         for i, (w, f, st, ev) in zip(idx, outs):
             if int(st[0]) == WDL_FIT_OVERFLOW:
-                host.append((i, "log", int(ev[0])))
+                logq[g].append((i, int(ev[0])))
             else:
                 results[i] = (w[0], float(f[0]), int(st[0]), int(ev[0]), "kernel")
-    if host:
-        # host-driven fits in worker threads, each with its own contexts (and
-        # so its own streams): the library calls release the interpreter lock,
-        # so the workers' launches overlap on the GPU
-        workers = max(1, min(host_workers, len(host)))
-        parts = [host[j::workers] for j in range(workers)]
-        with ThreadPoolExecutor(max_workers=workers) as ex:
-            outs = list(ex.map(lambda part: _fit_host(problems, part, lbfgs_iterations, device,
-                                                      epsilon), parts))
-        for part, res in zip(parts, outs):
-            for (i, _, spent), r in zip(part, res):
-                w, f, st, ev, dom = r
-                results[i] = (w, f, st, ev + spent, dom)
+    def log_fit(item):
+        g, todo = item
+        side = max(max(problems[i]["W"], problems[i]["H"]) for i, _ in todo)
+        kern = CudaLogSignArrayGaussian2DKernel(g, side, side, precision="fp32", device=device)
+        try:
+            return fit_device(kern, [problems[i] for i, _ in todo], lbfgs_iterations, epsilon,
+                              log_domain=True)
+        finally:
+            kern.close()
+
+    # one context (and stream) per gamma; the library calls release the
+    # interpreter lock, so the gammas' launches run concurrently on the GPU
+    items = list(logq.items())
+    with ThreadPoolExecutor(max_workers=max(1, len(items))) as ex:
+        outs_all = list(ex.map(log_fit, items))
+    for (g, todo), outs in zip(items, outs_all):
+        for (i, spent), (w, f, st, ev) in zip(todo, outs):
+            results[i] = (w[0], float(f[0]), int(st[0]), int(ev[0]) + spent, "log")
     return results
 
 

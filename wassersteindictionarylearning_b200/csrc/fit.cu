@@ -22,66 +22,35 @@
 #include <cstring>
 #include <vector>
 
+#include "lbfgs_dev.cuh"
 #include "wdl_internal.cuh"
 
 namespace wdl {
 namespace {
 
-constexpr int kM = 6;  // correction pairs (liblbfgs default, kept by the reference)
-
-// liblbfgs return codes (cpp/lbfgs/lbfgs.h:74-147)
-constexpr int kSuccess = 0, kAlreadyMinimized = 2, kMinimumStep = -1000, kMaximumStep = -999,
-              kMaximumLinesearch = -998, kMaximumIteration = -997, kInvalidParameters = -995,
-              kIncreaseGradient = -994;
-
-struct LbParam {
-  int max_iterations, max_linesearch;
-  double epsilon, ftol, wolfe, min_step, max_step;
-};
+using namespace lbdev;
 
 struct LbOpt {
-  int K, phase;  // phase: 0 first evaluation pending, 1 line-search trial pending, 2 done
-  int k, end, count, status, evals;
-  double f, finit, dginit, step, fret;
-  double* v;            // x, g, xp, gp, d [K each], s[m][K], y[m][K], ys[m], alpha[m]
+  LbState s;
+  double* v;            // state vectors (pool_doubles(K))
   double* lam64;        // the weights the fused kernel evaluates ([K], FP64 and FP32)
   float* lam32;
   const double* dot;    // weight gradient of that evaluation ([K], raw resultLa)
   const double* loss;   // its loss
 };
 
-inline size_t pool_doubles(int K) { return (size_t)(5 + 2 * kM) * K + 2 * kM; }
-
-__device__ void put_weights(const LbOpt& o, const double* x) {
-  double mx = x[0];
-  for (int k = 1; k < o.K; ++k) mx = x[k] > mx ? x[k] : mx;
-  double s = 0;
-  for (int k = 0; k < o.K; ++k) s += exp(x[k] - mx);
-  for (int k = 0; k < o.K; ++k) {
-    const double w = exp(x[k] - mx) / s;
-    o.lam64[k] = w;
-    o.lam32[k] = (float)w;
-  }
-}
-
-__device__ double dotk(const double* a, const double* b, int K) {
-  double s = 0;
-  for (int k = 0; k < K; ++k) s += a[k] * b[k];
-  return s;
-}
-
 __global__ void k_fit_init(LbOpt* opts, int n, const double* x0s) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   LbOpt o = opts[i];
   double* x = o.v;
-  for (int k = 0; k < o.K; ++k) x[k] = x0s ? x0s[(size_t)i * 64 + k] : 0.0;
-  put_weights(o, x);
+  for (int k = 0; k < o.s.K; ++k) x[k] = x0s ? x0s[(size_t)i * 64 + k] : 0.0;
+  softmax_weights(x, o.s.K, o.lam64, o.lam32);
 }
 
 // One optimisation step per histogram: consume the evaluation at the current
-// trial point, move to the next trial point (or finish).  Same decisions, in
-// the same order, as lbfgs_steps / liblbfgs.
+// trial point, move to the next trial point (or finish).  A non-finite
+// evaluation means the kernel domain overflowed at this point.
 __global__ void k_fit_round(LbOpt* opts, int n, LbParam prm, const int* fused_sync, int* sticky,
                             uint8_t* done) {
   __shared__ int s_err;
@@ -94,141 +63,10 @@ __global__ void k_fit_round(LbOpt* opts, int n, LbParam prm, const int* fused_sy
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   LbOpt o = opts[i];
-  if (o.phase == 2) return;
-  const int K = o.K;
-  double* x = o.v;
-  double* g = x + K;
-  double* xp = x + 2 * K;
-  double* gp = x + 3 * K;
-  double* d = x + 4 * K;
-  double* S = x + 5 * K;
-  double* Y = S + kM * K;
-  double* ys_h = Y + kM * K;
-  double* alpha = ys_h + kM;
-
-  o.evals++;
-  const double f = o.loss[0];
-  bool finite = isfinite(f);
-  double wla = 0;
-  for (int k = 0; k < K; ++k) {
-    finite = finite && isfinite(o.dot[k]);
-    wla += o.lam64[k] * o.dot[k];
-  }
-  auto finish = [&](int status, double fret) {
-    o.status = status;
-    o.fret = fret;
-    o.phase = 2;
-  };
-  if (!finite) {  // the kernel domain overflowed at this point
-    finish(WDL_FIT_OVERFLOW, f);
-    opts[i] = o;
-    done[i] = 1;
-    return;
-  }
-  for (int k = 0; k < K; ++k) g[k] = (o.dot[k] - wla) * o.lam64[k];
-
-  // start of a line search from the accepted point x (lbfgs.c:772-790)
-  auto start_ls = [&]() -> bool {
-    for (int k = 0; k < K; ++k) {
-      xp[k] = x[k];
-      gp[k] = g[k];
-    }
-    o.finit = o.f;
-    if (o.step <= 0) {
-      finish(kInvalidParameters, o.f);
-      return false;
-    }
-    o.dginit = dotk(g, d, K);
-    if (o.dginit > 0) {
-      finish(kIncreaseGradient, o.f);
-      return false;
-    }
-    o.count = 0;
-    for (int k = 0; k < K; ++k) x[k] = xp[k] + o.step * d[k];
-    put_weights(o, x);
-    o.phase = 1;
-    return true;
-  };
-
-  if (o.phase == 0) {  // first evaluation (lbfgs.c:423-470)
-    o.f = f;
-    const double xnorm = fmax(sqrt(dotk(x, x, K)), 1.0);
-    const double gnorm = sqrt(dotk(g, g, K));
-    if (gnorm / xnorm <= prm.epsilon) {
-      finish(kAlreadyMinimized, f);
-    } else {
-      for (int k = 0; k < K; ++k) d[k] = -g[k];
-      o.step = 1.0 / sqrt(dotk(d, d, K));
-      o.k = 1;
-      o.end = 0;
-      start_ls();
-    }
-  } else {  // a line-search trial (lbfgs.c:791-867)
-    o.count++;
-    double width = 0;
-    bool accept = false;
-    if (f > o.finit + o.step * prm.ftol * o.dginit) {
-      width = 0.5;
-    } else {
-      const double dg = dotk(g, d, K);
-      if (dg < prm.wolfe * o.dginit) width = 2.1;
-      else if (dg > -prm.wolfe * o.dginit) width = 0.5;
-      else accept = true;
-    }
-    if (!accept) {
-      int fail = 0;
-      if (o.step < prm.min_step) fail = kMinimumStep;
-      else if (o.step > prm.max_step) fail = kMaximumStep;
-      else if (prm.max_linesearch <= o.count) fail = kMaximumLinesearch;
-      if (fail) {  // revert to the previous point (lbfgs.c:487-492)
-        for (int k = 0; k < K; ++k) x[k] = xp[k];
-        finish(fail, o.finit);
-      } else {
-        o.step *= width;
-        for (int k = 0; k < K; ++k) x[k] = xp[k] + o.step * d[k];
-        put_weights(o, x);
-      }
-    } else {  // accepted: convergence tests, then the next direction (lbfgs.c:505-612)
-      o.f = f;
-      const double xnorm = sqrt(dotk(x, x, K));
-      const double gnorm = sqrt(dotk(g, g, K));
-      if (gnorm / fmax(xnorm, 1.0) <= prm.epsilon) {
-        finish(kSuccess, f);
-      } else if (prm.max_iterations != 0 && prm.max_iterations < o.k + 1) {
-        finish(kMaximumIteration, f);
-      } else {
-        double* s_e = S + (size_t)o.end * K;
-        double* y_e = Y + (size_t)o.end * K;
-        for (int k = 0; k < K; ++k) {
-          s_e[k] = x[k] - xp[k];
-          y_e[k] = g[k] - gp[k];
-        }
-        const double ys = dotk(y_e, s_e, K);
-        const double yy = dotk(y_e, y_e, K);
-        ys_h[o.end] = ys;
-        const int bound = o.k < kM ? o.k : kM;
-        o.k++;
-        o.end = (o.end + 1) % kM;
-        for (int k = 0; k < K; ++k) d[k] = -g[k];
-        int j = o.end;
-        for (int b = 0; b < bound; ++b) {
-          j = (j + kM - 1) % kM;
-          alpha[j] = dotk(S + (size_t)j * K, d, K) / ys_h[j];
-          for (int k = 0; k < K; ++k) d[k] -= alpha[j] * Y[(size_t)j * K + k];
-        }
-        for (int k = 0; k < K; ++k) d[k] *= ys / yy;
-        for (int b = 0; b < bound; ++b) {
-          const double beta = dotk(Y + (size_t)j * K, d, K) / ys_h[j];
-          for (int k = 0; k < K; ++k) d[k] += (alpha[j] - beta) * S[(size_t)j * K + k];
-          j = (j + 1) % kM;
-        }
-        o.step = 1.0;
-        start_ls();
-      }
-    }
-  }
+  if (o.s.phase == 2) return;
+  lbfgs_advance(o.s, o.v, o.loss[0], o.dot, o.lam64, o.lam32, prm, WDL_FIT_OVERFLOW);
   opts[i] = o;
-  done[i] = o.phase == 2 ? 1 : 0;
+  done[i] = o.s.phase == 2 ? 1 : 0;
 }
 
 struct FitOut {
@@ -241,15 +79,10 @@ __global__ void k_fit_outputs(const LbOpt* opts, int n, FitOut* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const LbOpt o = opts[i];
-  const double* x = o.v;
-  double mx = x[0];
-  for (int k = 1; k < o.K; ++k) mx = x[k] > mx ? x[k] : mx;
-  double s = 0;
-  for (int k = 0; k < o.K; ++k) s += exp(x[k] - mx);
-  for (int k = 0; k < o.K; ++k) out[i].w[k] = exp(x[k] - mx) / s;
-  out[i].loss = o.phase == 2 ? o.fret : o.f;
-  out[i].status = o.phase == 2 ? o.status : kMaximumIteration;
-  out[i].evals = o.evals;
+  softmax_weights(o.v, o.s.K, out[i].w, nullptr);
+  out[i].loss = o.s.phase == 2 ? o.s.fret : o.s.f;
+  out[i].status = o.s.phase == 2 ? o.s.status : kMaximumIteration;
+  out[i].evals = o.s.evals;
 }
 
 inline size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -324,7 +157,7 @@ extern "C" int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* fp, int npro
       const BatchBuf& b = bp.buf[q];
       for (int p = 0; p < f.P; ++p, ++i) {
         LbOpt o{};
-        o.K = f.K;
+        o.s.K = f.K;
         o.v = d_pool + po;
         po += pool_doubles(f.K);
         o.lam64 = b.lam64 + (size_t)p * f.K;
