@@ -534,10 +534,65 @@ def run_uneven(args):
     print(json.dumps(line), flush=True)
 
 
+def run_uneven_reference(args):
+    """The reference's own CPU path on the uneven workload: it fits one problem
+    at a time, each L-BFGS evaluation one evaluate_both (log domain, the
+    domain the workload needs; LogSignArrayGaussian2DKernel, OpenMP over all
+    host cores).  Bounded sample: one evaluation of each of the two problems
+    of median operator work (K L N (W + H)); the whole workload's time is that
+    rate times the workload's total work, times the 14.9 evaluations per fit
+    our run of the same problems used."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+
+    from oracle import oracle as orc
+    from wassersteindictionarylearning_b200.batch import uneven_problems
+    from wassersteindictionarylearning_b200.synthetic import to_variables
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+    lib = orc.RefLib()
+    probs = uneven_problems(n=512, seed=0)
+    work = [pr["K"] * pr["L"] * pr["W"] * pr["H"] * (pr["W"] + pr["H"]) for pr in probs]
+    order = sorted(range(len(probs)), key=lambda i: work[i])
+    sample = [order[len(order) // 2 - 1], order[len(order) // 2]]
+    t_sample, w_sample = 0.0, 0.0
+    for i in sample:
+        pr = probs[i]
+        W, H, K, L, g = pr["W"], pr["H"], pr["K"], pr["L"], pr["gamma"]
+        a = pr["atoms"].reshape(K, -1)
+        x = to_variables(np.ones((1, K)) / K, a / a.sum(axis=1, keepdims=True), 1.0)
+        t0 = time.perf_counter()
+        lib.evaluate_both(W, H, 1, g, 1, K, L, pr.get("loss_type", 2), 1.0, x, pr["observed"],
+                          log_domain=True)
+        t_sample += time.perf_counter() - t0
+        w_sample += work[i]
+    evals_per_fit = 14.9
+    total = sum(work) / w_sample * t_sample * evals_per_fit
+    value = len(probs) / total
+    desc = ", ".join(f"{probs[i]['W']}x{probs[i]['H']} K={probs[i]['K']} L={probs[i]['L']}" for i in sample)
+    line = dict(metric="weight fits/s (uneven 512-problem batch)", value=value, unit="fits/s",
+                n_gpus=args.gpus, steps=1, warmup=0, ms_per_step=total * 1e3, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload="uneven512", note="bounded sample of the workload, scaled by work"),
+                impl="reference",
+                cpu_baseline=dict(value=value, unit="fits/s", cores=lib.omp_threads(), kind="reference",
+                                  sample=f"LogSignArrayGaussian2DKernel evaluate_both "
+                                         f"(cpp/inverseWasserstein.h:986), OpenMP; one evaluation each "
+                                         f"of the 2 median-work problems ({desc}), {t_sample:.2f} s, "
+                                         f"scaled to the 512 problems' work x {evals_per_fit} "
+                                         f"evaluations per fit; CPU: {cpu_model()}"),
+                e2e=dict(value=value, unit="fits/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "uneven512":
-        run_uneven(args)
+        if args.impl == "reference":
+            run_uneven_reference(args)
+        else:
+            run_uneven(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
