@@ -392,8 +392,10 @@ def run_ours(args):
                         executed_tflops=achieved_tflops * products,
                         ceiling_frac=1.0 / products,
                         kernel=(f"fused Sinkhorn kernel: one launch = {imgs_per_launch:.0f} separable-operator "
-                                "applications (whole forward + reverse pass)" if precision in ("split_bf16", "tf32")
-                                else f"separable Gaussian operator: one launch = {imgs_per_launch:.0f} images"),
+                                "applications (whole forward + reverse pass)"
+                                if precision in ("split_bf16", "tf32") and W <= 128 and H <= 128
+                                else f"separable Gaussian operator ({'tensor-core axis passes' if precision in ('split_bf16', 'tf32') else 'CUDA cores'}): "
+                                     f"one launch = {imgs_per_launch:.0f} images"),
                         conv_share_of_step=conv_ms.value / (ms / args.steps))
 
     # End to end through the public host-pointer API (pinned host buffers).
