@@ -55,36 +55,49 @@ __device__ __forceinline__ void put_axis_chunk(uint8_t* tile, int r, int k0, con
   }
 }
 
-// Rows row0.. (at most `rows` valid) of a row-major matrix with `len` elements
-// per row, elements kb..kb+63 (zero beyond len), into a 128 x 64 operand.
+// Rows 0.. (at most `rows` valid) of a row-major matrix with `len` elements
+// per row, elements kb..kb+63 (zero beyond len): loaded into registers by
+// load_operand, converted and stored into a 128 x 64 operand by
+// store_operand, so the loads of the next chunk can be in flight while the
+// current one is converted and multiplied.
 template <bool SPLIT>
-__device__ __forceinline__ void stage_operand(uint8_t* tile, const float* __restrict__ src, int rows,
-                                              int len, int kb, bool vec, int t) {
-  constexpr int CE = SPLIT ? 8 : 4;
-  constexpr int CPR = kAxKc / CE;            // chunks per row
-  constexpr int PER = kAxTile * CPR / kAxThreads;  // chunks per thread
+struct OperandRegs {
+  static constexpr int CE = SPLIT ? 8 : 4;
+  static constexpr int CPR = kAxKc / CE;                 // chunks per row
+  static constexpr int PER = kAxTile * CPR / kAxThreads;  // chunks per thread
   float v[PER][CE];
+};
+
+template <bool SPLIT>
+__device__ __forceinline__ void load_operand(OperandRegs<SPLIT>& o, const float* __restrict__ src, int rows,
+                                             int len, int kb, bool vec, int t) {
+  using O = OperandRegs<SPLIT>;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
+  for (int u = 0; u < O::PER; ++u) {
     const int c = t + u * kAxThreads;
-    const int r = c / CPR, k0 = kb + (c - r * CPR) * CE;
+    const int r = c / O::CPR, k0 = kb + (c - r * O::CPR) * O::CE;
     const float* row = src + (size_t)r * len;
-    if (r < rows && vec && k0 + CE <= len) {
+    if (r < rows && vec && k0 + O::CE <= len) {
 #pragma unroll
-      for (int q = 0; q < CE; q += 4) {
+      for (int q = 0; q < O::CE; q += 4) {
         const float4 f = __ldg(reinterpret_cast<const float4*>(row + k0 + q));
-        v[u][q] = f.x; v[u][q + 1] = f.y; v[u][q + 2] = f.z; v[u][q + 3] = f.w;
+        o.v[u][q] = f.x; o.v[u][q + 1] = f.y; o.v[u][q + 2] = f.z; o.v[u][q + 3] = f.w;
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < CE; ++q) v[u][q] = (r < rows && k0 + q < len) ? __ldg(row + k0 + q) : 0.f;
+      for (int q = 0; q < O::CE; ++q) o.v[u][q] = (r < rows && k0 + q < len) ? __ldg(row + k0 + q) : 0.f;
     }
   }
+}
+
+template <bool SPLIT>
+__device__ __forceinline__ void store_operand(uint8_t* tile, const OperandRegs<SPLIT>& o, int t) {
+  using O = OperandRegs<SPLIT>;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
+  for (int u = 0; u < O::PER; ++u) {
     const int c = t + u * kAxThreads;
-    const int r = c / CPR, kk = (c - r * CPR) * CE;
-    put_axis_chunk<SPLIT>(tile, r, kk, v[u]);
+    const int r = c / O::CPR, kk = (c - r * O::CPR) * O::CE;
+    put_axis_chunk<SPLIT>(tile, r, kk, o.v[u]);
   }
 }
 
@@ -146,6 +159,8 @@ __global__ void __launch_bounds__(kAxThreads, 1)
   using F = Fmt<SPLIT>;
   const uint32_t id = ptx::idesc(F::fmt, 128, 128);
   bool ok = true;
+  OperandRegs<SPLIT> breg;
+  load_operand<SPLIT>(breg, src, b_rows, C, 0, vec, t);
   for (int j = 0; j < nch; ++j) {
     const int st = j & 1;
     uint8_t* a_tile = base + st * kAxStage;
@@ -165,7 +180,8 @@ __global__ void __launch_bounds__(kAxThreads, 1)
       }
       cp_async_commit();
     }
-    stage_operand<SPLIT>(b_tile, src, b_rows, C, j * kAxKc, vec, t);
+    store_operand<SPLIT>(b_tile, breg, t);
+    if (j + 1 < nch) load_operand<SPLIT>(breg, src, b_rows, C, (j + 1) * kAxKc, vec, t);
     cp_async_wait_all();
     ptx::fence_proxy_async_smem();
     ptx::tc_fence_before();
