@@ -168,15 +168,41 @@ __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&s
 
 struct Ctl {
   uint8_t* tile;
-  uint32_t g_a, x_a, bar_a, d1, d2, lane_base;
+  uint32_t g_a, x_a, bar_a, d1, d2, a_hi, a_lo, lane_base;
   int st, t, lane_row, half;
   uint32_t phase;
 };
 
+// D[128 x N] = A[128 x K] * B[N x K]^T with A in tensor memory (lane = row,
+// K along the columns: BF16 pairs or TF32 values, hi and lo planes for split
+// BF16) and B a K-major SMEM tile.
+template <bool SPLIT>
+__device__ __forceinline__ void issue_gemm_ta(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_tile,
+                                              int K, int N) {
+  using F = Fmt<SPLIT>;
+  const uint32_t id = ptx::idesc(F::fmt, 128, (uint32_t)N);
+  const int steps = K / F::kstep;
+  for (int ks = 0; ks < steps; ++ks) {
+    const uint32_t byte = (uint32_t)ks * 32u;
+    const uint32_t off = (byte >> 7) * kRegionBytes + (byte & 127u);
+    const uint64_t b = ptx::sw128_desc(b_tile + off);
+    const uint32_t col = (uint32_t)ks * 8u;  // 16 BF16 or 8 TF32 values
+    if (SPLIT) {
+      const uint64_t blo = ptx::sw128_desc(b_tile + F::plane_bytes + off);
+      ptx::mma_bf16_ta(d_tmem, a_hi + col, b, id, ks > 0 ? 1u : 0u);
+      ptx::mma_bf16_ta(d_tmem, a_hi + col, blo, id, 1u);
+      ptx::mma_bf16_ta(d_tmem, a_lo + col, b, id, 1u);
+    } else {
+      ptx::mma_tf32_ta(d_tmem, a_hi + col, b, id, ks > 0 ? 1u : 0u);
+    }
+  }
+}
+
 // Separable convolution of the operand tile: MMA1 (A = G, B = tile rows n, K =
-// K1) -> D1 -> restaged as the A operand (row = this thread's lane; warps w and
-// w+4 of the stream take alternate 16-column chunks of the same lanes) -> MMA2
-// (B = G) -> D2.  Column form: K1 = Wp, N1 = Hp; row form: K1 = Hp, N1 = Wp.
+// K1) -> D1 -> restaged in tensor memory as the A operand (row = this thread's
+// lane; warps w and w+4 of the stream take alternate 16-column chunks of the
+// same lanes) -> MMA2 (A from tensor memory, B = G) -> D2 in D1's columns.
+// Column form: K1 = Wp, N1 = Hp; row form: K1 = Hp, N1 = Wp.
 template <bool SPLIT>
 __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
   ptx::tc_fence_before();
@@ -190,18 +216,37 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
   bool ok = bar_all(ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
   c.phase ^= 1;
   ptx::tc_fence_after();
+  // D1 -> the second GEMM's A operand, kept in tensor memory (split into BF16
+  // hi / lo, or rounded to TF32); the second GEMM then overwrites D1's columns
   for (int c0 = 16 * c.half; c0 < N1; c0 += 32) {
     float v[16];
     ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, v);
     ptx::tmem_ld_wait();
-    put16<SPLIT>(c.tile, c.lane_row, c0, v);
+    if (SPLIT) {
+      uint32_t hi[8], lo[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
+        hi[q] = *reinterpret_cast<const uint32_t*>(&h);
+        lo[q] = *reinterpret_cast<const uint32_t*>(&l);
+      }
+      ptx::tmem_st8(c.a_hi + c.lane_base + (uint32_t)(c0 >> 1), hi);
+      ptx::tmem_st8(c.a_lo + c.lane_base + (uint32_t)(c0 >> 1), lo);
+    } else {
+      uint32_t r[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) r[q] = to_tf32(v[q]);
+      ptx::tmem_st16(c.a_hi + c.lane_base + (uint32_t)c0, r);
+    }
   }
+  ptx::tmem_st_wait();
   ptx::tc_fence_before();
-  ptx::fence_proxy_async_smem();
   bar_sync(c.st, kSt);
   if (c.t == 0) {
     ptx::tc_fence_after();
-    issue_gemm<SPLIT>(c.d2, c.x_a, c.g_a, N1, N1);
+    issue_gemm_ta<SPLIT>(c.d2, c.a_hi, c.a_lo, c.g_a, N1, N1);
     ptx::mma_commit(c.bar_a);
   }
   ok = bar_all(ok && ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
@@ -358,8 +403,12 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   c.g_a = ptx::smem_addr(g_tile);
   c.x_a = ptx::smem_addr(c.tile);
   c.bar_a = ptx::smem_addr(&bars[st]);
+  // per stream: D1 and D2 share columns [0, 128), the second GEMM's A operand
+  // in tensor memory takes [128, 256) (BF16 hi [128, 192), lo [192, 256))
   c.d1 = *tmem_slot + (uint32_t)st * kTmemCols;
-  c.d2 = c.d1 + 128;
+  c.d2 = c.d1;
+  c.a_hi = c.d1 + 128;
+  c.a_lo = c.d1 + 192;
   c.lane_base = (uint32_t)((ws & 3) * 32) << 16;
   c.st = st;
   c.t = t;
