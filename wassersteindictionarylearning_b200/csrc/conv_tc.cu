@@ -5,18 +5,19 @@
 // dense symmetric Gibbs factors (cpp/kernels.h:669-699).  One CTA computes a
 // whole image with two tcgen05 GEMMs (M = 128 lanes = the x coordinate j):
 //   MMA1: D1[j][i] = sum_k G[j][k] U[i][k]   (A = G, B = U; both K-major in SMEM)
-//   MMA2: D2[j][i] = sum_m D1[j][m] G[i][m]  (A = D1 restaged to SMEM, B = G)
-// so D2[j][i] = out[i][j].  D1 goes TMEM -> registers -> SMEM (as the next
-// GEMM's K-major A operand) without leaving the SM, and D2 is read back with
-// tcgen05.ld in which a warp's 32 lanes are 32 consecutive x: every global
-// store of the epilogue is a coalesced 128-byte row segment.
+//   MMA2: D2[j][i] = sum_m D1[j][m] G[i][m]  (A = D1 restaged in TMEM, B = G)
+// so D2[j][i] = out[i][j].  D1 goes TMEM -> registers -> TMEM (split into
+// BF16 hi / lo, or rounded to TF32) as the next GEMM's A operand, which
+// tcgen05.mma reads from tensor memory, and D2 is read back with tcgen05.ld in
+// which a warp's 32 lanes are 32 consecutive x: every global store of the
+// epilogue is a coalesced 128-byte row segment.
 //
 // Precision: kind::tf32 (operands rounded to TF32, FP32 accumulate) or split
 // BF16 (x = hi + lo, both BF16; hi*hi + hi*lo + lo*hi accumulated in FP32 with
 // kind::f16), the latter ~2^-16 relative per product.
 //
 // Shared memory holds the factor G (resident for the CTA's lifetime) and one
-// operand tile that is reused for U and for the restaged D1: 128 KB.  Operand
+// operand tile per warpgroup for U.  Operand
 // tiles use the canonical 128-byte-swizzled K-major layout: a tile of 128 rows
 // is split along K into 128-byte column blocks ("regions") of 128 x 128 B; in a
 // region, row r's 16-byte chunk c sits at chunk position c ^ (r % 8).
@@ -98,7 +99,8 @@ __device__ __forceinline__ void stage_image(uint8_t* tile, const float* __restri
 // Two warpgroups per CTA, each streaming its own images through the shared
 // tensor pipe (while one restages or stores, the other's GEMM runs).  Warp w
 // of warpgroup g owns TMEM lanes 32(w%4)..+31; slot g uses TMEM columns
-// [256g, 256g+256): D1 at +0, D2 at +128.  The factor tile G is shared.
+// [256g, 256g+256): D1 and then D2 at +0, the restaged A operand at +128.
+// The factor tile G is shared.
 template <bool SPLIT>
 __global__ void __launch_bounds__(256, 1)
     tc_conv2d_kernel(const float* __restrict__ in, float* __restrict__ out, long long nimg, int W,
@@ -127,7 +129,8 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t tmem = *tmem_slot + (uint32_t)wg * kTmemCols;
-  const uint32_t d1 = tmem, d2 = tmem + 128;
+  // D1 and D2 share [0, 128); the second GEMM's A operand lives in [128, 256)
+  const uint32_t d1 = tmem, d2 = tmem, a_hi = tmem + 128, a_lo = tmem + 192;
   const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   const int j = (warp & 3) * 32 + lane;  // x coordinate owned by this thread
   const bool vec = (W % 4) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0;
@@ -148,19 +151,19 @@ __global__ void __launch_bounds__(256, 1)
     ok = wg_all(ptx::mbar_wait(bar_a, phase, kWaitNs), wg);
     phase ^= 1;
     ptx::tc_fence_after();
-    // D1 -> SMEM as the K-major A operand of the second GEMM (row j, K = i).
+    // D1 -> the second GEMM's A operand (row j, K = i), kept in tensor memory
     for (int c0 = 0; c0 < Hp; c0 += 16) {
       float v[16];
       ptx::tmem_ld16(d1 + lane_base + (uint32_t)c0, v);
       ptx::tmem_ld_wait();
-      put16<SPLIT>(x_tile, j, c0, v);
+      restage16_tmem<SPLIT>(a_hi, a_lo, lane_base, c0, v);
     }
+    ptx::tmem_st_wait();
     ptx::tc_fence_before();
-    ptx::fence_proxy_async_smem();
     wg_sync(wg);
     if (wt == 0) {
       ptx::tc_fence_after();
-      issue_gemm<SPLIT>(d2, x_a, g_a, Hp, Hp);
+      issue_gemm_ta<SPLIT>(d2, a_hi, a_lo, g_a, Hp, Hp);
       ptx::mma_commit(bar_a);
     }
     ok = wg_all(ok && ptx::mbar_wait(bar_a, phase, kWaitNs), wg);

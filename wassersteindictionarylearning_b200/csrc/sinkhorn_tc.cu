@@ -173,31 +173,6 @@ struct Ctl {
   uint32_t phase;
 };
 
-// D[128 x N] = A[128 x K] * B[N x K]^T with A in tensor memory (lane = row,
-// K along the columns: BF16 pairs or TF32 values, hi and lo planes for split
-// BF16) and B a K-major SMEM tile.
-template <bool SPLIT>
-__device__ __forceinline__ void issue_gemm_ta(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_tile,
-                                              int K, int N) {
-  using F = Fmt<SPLIT>;
-  const uint32_t id = ptx::idesc(F::fmt, 128, (uint32_t)N);
-  const int steps = K / F::kstep;
-  for (int ks = 0; ks < steps; ++ks) {
-    const uint32_t byte = (uint32_t)ks * 32u;
-    const uint32_t off = (byte >> 7) * kRegionBytes + (byte & 127u);
-    const uint64_t b = ptx::sw128_desc(b_tile + off);
-    const uint32_t col = (uint32_t)ks * 8u;  // 16 BF16 or 8 TF32 values
-    if (SPLIT) {
-      const uint64_t blo = ptx::sw128_desc(b_tile + F::plane_bytes + off);
-      ptx::mma_bf16_ta(d_tmem, a_hi + col, b, id, ks > 0 ? 1u : 0u);
-      ptx::mma_bf16_ta(d_tmem, a_hi + col, blo, id, 1u);
-      ptx::mma_bf16_ta(d_tmem, a_lo + col, b, id, 1u);
-    } else {
-      ptx::mma_tf32_ta(d_tmem, a_hi + col, b, id, ks > 0 ? 1u : 0u);
-    }
-  }
-}
-
 // Separable convolution of the operand tile: MMA1 (A = G, B = tile rows n, K =
 // K1) -> D1 -> restaged in tensor memory as the A operand (row = this thread's
 // lane; warps w and w+4 of the stream take alternate 16-column chunks of the
@@ -222,24 +197,7 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
     float v[16];
     ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, v);
     ptx::tmem_ld_wait();
-    if (SPLIT) {
-      uint32_t hi[8], lo[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-        const float2 hf = __bfloat1622float2(h);
-        const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * q] - hf.x, v[2 * q + 1] - hf.y);
-        hi[q] = *reinterpret_cast<const uint32_t*>(&h);
-        lo[q] = *reinterpret_cast<const uint32_t*>(&l);
-      }
-      ptx::tmem_st8(c.a_hi + c.lane_base + (uint32_t)(c0 >> 1), hi);
-      ptx::tmem_st8(c.a_lo + c.lane_base + (uint32_t)(c0 >> 1), lo);
-    } else {
-      uint32_t r[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) r[q] = to_tf32(v[q]);
-      ptx::tmem_st16(c.a_hi + c.lane_base + (uint32_t)c0, r);
-    }
+    restage16_tmem<SPLIT>(c.a_hi, c.a_lo, c.lane_base, c0, v);
   }
   ptx::tmem_st_wait();
   ptx::tc_fence_before();
