@@ -197,7 +197,8 @@ int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* problems, int nproblems
  * and the weight recursion), for problems whose kernel-domain scalings leave
  * the float range: ONE persistent launch in which every histogram's whole
  * L-BFGS fit runs on the device (one CTA per histogram up to sides of 32, a
- * cluster of 2, 4 or 8 CTAs up to 64, 128, 512).  Context: 2-D,
+ * cluster of 2, 4 or 16 CTAs up to 64, 128, 512; 8 where the GPU cannot
+ * place 16-CTA clusters).  Context: 2-D,
  * WDL_DOMAIN_LOG, FP32 arithmetic;
  * its gamma serves every problem.  Sides <= 512, K <= 16, loss 1, 2 or 4.
  * status[p] is liblbfgs' return code, or WDL_ERR_NONFINITE if an evaluation

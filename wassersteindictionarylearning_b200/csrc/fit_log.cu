@@ -10,7 +10,7 @@
 // (lbfgs_dev.cuh), as regress_both runs it around evaluate_both.
 //
 // Each problem gets a group of CTAs by its size: 1 (sides <= 32), a cluster of
-// 2 (<= 64), 4 (<= 128) or 8 (above); a cluster splits every pass's rows and
+// 2 (<= 64), 4 (<= 128) or 16 (above); a cluster splits every pass's rows and
 // every elementwise loop and meets at cluster barriers.  The four classes run
 // as four launches on their own streams, concurrently.  A group never waits
 // on another group, so the launch needs no residency guarantee and has no
@@ -35,8 +35,10 @@ namespace {
 using namespace lbdev;
 
 constexpr int kLfThreads = 256;
-constexpr int kLfRows = 16;      // rows per pass block
-constexpr int kGroups[4] = {1, 2, 4, 8};  // CTAs per problem, by size class
+// CTAs per problem and rows per pass block, by size class; the largest class
+// uses 16-CTA clusters (a non-portable size, falling back to 8) with 8-row
+// blocks, so that a 192-row pass still gives every CTA rows.
+constexpr int kGroups[4] = {1, 2, 4, 16};
 inline int size_class(int W, int H) {
   const int m = W > H ? W : H;
   return m <= 32 ? 0 : m <= 64 ? 1 : m <= 128 ? 2 : 3;
@@ -96,22 +98,22 @@ __device__ double block_sum_d(double v, double* sh) {
 // rows shared among the group: out[c][r] = log sum_k s_k exp(-(c-k)^2/gamma +
 // in[r][k]) (signs optional, in and out sign arrays distinct), as the
 // CUDA-core operator's pass but with the maximum and the sum in one pass.
-template <bool SIGNED, int G>
+template <bool SIGNED, int G, int LR>
 __device__ void lse_pass(const float* __restrict__ in, float* __restrict__ out, int R, int C, float gamma,
                          const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign, float* sm,
                          int rank) {
   const int CP = C + 1, SP = C + 4;
   float* rows = sm;
-  float* lk = rows + kLfRows * CP;
+  float* lk = rows + LR * CP;
   float* xmax = lk + C;
-  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + kLfRows);
+  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   __syncthreads();
   for (int d = tid; d < C; d += kLfThreads) lk[d] = -float(d) * float(d) / gamma * kLog2e;
-  for (int rb = rank; rb * kLfRows < R; rb += G) {
-    const int r0 = rb * kLfRows, nr = min(kLfRows, R - r0);
+  for (int rb = rank; rb * LR < R; rb += G) {
+    const int r0 = rb * LR, nr = min(LR, R - r0);
     __syncthreads();
-    for (int rr = warp; rr < kLfRows; rr += kLfThreads / 32) {
+    for (int rr = warp; rr < LR; rr += kLfThreads / 32) {
       float vm = kFloorF;
       for (int k = lane; k < C; k += 32) {
         float v = kFloorF;
@@ -131,8 +133,8 @@ __device__ void lse_pass(const float* __restrict__ in, float* __restrict__ out, 
       if (lane == 0) xmax[rr] = vm;
     }
     __syncthreads();
-    for (int e = tid; e < kLfRows * C; e += kLfThreads) {
-      const int c = e / kLfRows, rr = e - c * kLfRows;
+    for (int e = tid; e < LR * C; e += kLfThreads) {
+      const int c = e / LR, rr = e - c * LR;
       if (rr >= nr) continue;
       const float* row = rows + rr * CP;
       const float X = xmax[rr];
@@ -184,16 +186,16 @@ __device__ void lse_pass(const float* __restrict__ in, float* __restrict__ out, 
 }
 
 // The 2-D operator: x pass into t1 (transposed), y pass into out.
-template <bool SIGNED, int G>
+template <bool SIGNED, int G, int LR>
 __device__ void lse_image(const float* in, float* out, const LogFitProblem& p, float gamma, uint8_t* signs,
                           float* sm, int rank) {
-  lse_pass<SIGNED, G>(in, p.t1, p.H, p.W, gamma, signs, p.ts, sm, rank);
+  lse_pass<SIGNED, G, LR>(in, p.t1, p.H, p.W, gamma, signs, p.ts, sm, rank);
   group_sync<G>();
-  lse_pass<SIGNED, G>(p.t1, out, p.W, p.H, gamma, p.ts, signs, sm, rank);
+  lse_pass<SIGNED, G, LR>(p.t1, out, p.W, p.H, gamma, p.ts, signs, sm, rank);
   group_sync<G>();
 }
 
-template <int G>
+template <int G, int LR>
 __global__ void __launch_bounds__(kLfThreads)
     log_fit_kernel(const LogFitProblem* __restrict__ probs, int nprob, LbParam prm, float gamma, int max_evals) {
   extern __shared__ float sm[];
@@ -223,10 +225,10 @@ __global__ void __launch_bounds__(kLfThreads)
       float* cb = p.tcb + (size_t)(it - 1) * KN;
       float* ph = p.tphi + (size_t)(it - 1) * KN;
       for (int k = 0; k < K; ++k) {
-        lse_image<false, G>(bprev + k * N, cb + k * N, p, gamma, nullptr, sm, rank);
+        lse_image<false, G, LR>(bprev + k * N, cb + k * N, p, gamma, nullptr, sm, rank);
         for (size_t j = g0; j < N; j += gstride) p.a[j] = p.latoms[k * N + j] - cb[k * N + j];
         group_sync<G>();
-        lse_image<false, G>(p.a, ph + k * N, p, gamma, nullptr, sm, rank);
+        lse_image<false, G, LR>(p.a, ph + k * N, p, gamma, nullptr, sm, rank);
       }
       float* bnext = p.tb + (size_t)it * KN;
       for (size_t j = g0; j < N; j += gstride) {
@@ -286,11 +288,11 @@ __global__ void __launch_bounds__(kLfThreads)
       const float* cbs = p.tcb + (size_t)(s - 1) * KN;
       const float* bp = p.tb + (size_t)(s - 1) * KN;
       for (int k = 0; k < K; ++k) {
-        lse_image<true, G>(p.u + k * N, p.a, p, gamma, p.sw + k * N, sm, rank);
+        lse_image<true, G, LR>(p.u + k * N, p.a, p, gamma, p.sw + k * N, sm, rank);
         for (size_t j = g0; j < N; j += gstride)
           p.u[k * N + j] = p.a[j] + (p.latoms[k * N + j] - 2.f * cbs[k * N + j]);
         group_sync<G>();
-        lse_image<true, G>(p.u + k * N, p.a, p, gamma, p.sw + k * N, sm, rank);
+        lse_image<true, G, LR>(p.u + k * N, p.a, p, gamma, p.sw + k * N, sm, rank);
         for (size_t j = g0; j < N; j += gstride) {
           const float ex = expf(p.a[j] + bp[k * N + j]);
           p.r[k * N + j] = p.sw[k * N + j] ? ex : -ex;
@@ -328,17 +330,19 @@ __global__ void __launch_bounds__(kLfThreads)
 
 inline size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
-size_t lse_smem(int C) {
-  return ((size_t)kLfRows * (C + 1) + C + kLfRows) * sizeof(float) + (size_t)kLfRows * (C + 4) + 16;
+size_t lse_smem(int C, int LR) {
+  return ((size_t)LR * (C + 1) + C + LR) * sizeof(float) + (size_t)LR * (C + 4) + 16;
 }
 
-template <int G>
+template <int G, int LR>
 int launch_log_fit(wdl_ctx* ctx, const LogFitProblem* d_probs, int n, const LbParam& prm, int max_evals,
                    int maxC, cudaStream_t s) {
-  const size_t smem = lse_smem(maxC);
-  auto kern = log_fit_kernel<G>;
+  const size_t smem = lse_smem(maxC, LR);
+  auto kern = log_fit_kernel<G, LR>;
   if (smem > 48 * 1024)
     WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (G > 8)
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   if (G == 1) {
     kern<<<n, kLfThreads, smem, s>>>(d_probs, n, prm, (float)ctx->gamma, max_evals);
   } else {
@@ -358,6 +362,36 @@ int launch_log_fit(wdl_ctx* ctx, const LogFitProblem* d_probs, int n, const LbPa
   }
   WDL_LAUNCH_CHECK(ctx);
   return WDL_OK;
+}
+
+// Whether a 16-CTA cluster of this kernel can be resident at all (a
+// non-portable size; otherwise the class runs on 8-CTA clusters).
+bool big_clusters_fit(size_t smem) {
+  auto kern = log_fit_kernel<16, 8>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      (smem > 48 * 1024 &&
+       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(16);
+  cfg.blockDim = dim3(kLfThreads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 16;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return nclusters > 0;
 }
 
 }  // namespace
@@ -531,10 +565,16 @@ extern "C" int wdl_fit_weights_log(wdl_ctx* ctx, const wdl_fit_problem* fp, int 
         }
         const LogFitProblem* dp = d_probs + first;
         switch (cls) {
-          case 0: rc = launch_log_fit<1>(ctx, dp, cnt[0], prm, max_evals, maxC[0], cs[0]); break;
-          case 1: rc = launch_log_fit<2>(ctx, dp, cnt[1], prm, max_evals, maxC[1], cs[1]); break;
-          case 2: rc = launch_log_fit<4>(ctx, dp, cnt[2], prm, max_evals, maxC[2], cs[2]); break;
-          default: rc = launch_log_fit<8>(ctx, dp, cnt[3], prm, max_evals, maxC[3], cs[3]); break;
+          case 0: rc = launch_log_fit<1, 16>(ctx, dp, cnt[0], prm, max_evals, maxC[0], cs[0]); break;
+          case 1: rc = launch_log_fit<2, 16>(ctx, dp, cnt[1], prm, max_evals, maxC[1], cs[1]); break;
+          case 2: rc = launch_log_fit<4, 16>(ctx, dp, cnt[2], prm, max_evals, maxC[2], cs[2]); break;
+          default:
+            if (big_clusters_fit(lse_smem(maxC[3], 8))) {
+              rc = launch_log_fit<16, 8>(ctx, dp, cnt[3], prm, max_evals, maxC[3], cs[3]);
+            } else {
+              rc = launch_log_fit<8, 16>(ctx, dp, cnt[3], prm, max_evals, maxC[3], cs[3]);
+            }
+            break;
         }
         first += cnt[cls];
       }
