@@ -332,8 +332,13 @@ def run_ours(args):
     key6, choice, tms = (C.c_longlong * 6)(), C.c_int(), C.c_float()
     for i in range(max(L_.wdl_autotune_count(ctx), 0)):
         if L_.wdl_autotune_entry(ctx, i, key6, C.byref(choice), C.byref(tms)) == 0:
-            tuned.append(dict(rows=key6[1], row_len=key6[2], images=key6[3], signed=bool(key6[5]),
-                              rows_per_block=choice.value, ms=round(tms.value, 4)))
+            if key6[0] == 2:  # tensor-core axis pass: output tile height
+                tuned.append(dict(kind="tc_axis_pass", rows=key6[1], row_len=key6[2], images=key6[3],
+                                  tile_rows=choice.value, ms=round(tms.value, 4)))
+            else:  # log-domain axis pass: rows per block
+                tuned.append(dict(kind="log_axis_pass", rows=key6[1], row_len=key6[2], images=key6[3],
+                                  signed=bool(key6[5]), rows_per_block=choice.value,
+                                  ms=round(tms.value, 4)))
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))

@@ -63,3 +63,38 @@ def test_split_bf16_evaluate_beyond_one_tile(oracle, shape):
     scale = oracle.weight_gradient_scale(W, H, D, gamma, P, K, L, loss, sd, x, obs)
     assert rel_scaled(g[:PK], g_ref[:PK], scale) < 1e-3
     k.close()
+
+
+@pytest.mark.parametrize("shape", [(272, 240, 1), (129, 200, 1), (40, 33, 20)])
+@pytest.mark.parametrize("precision", ["split_bf16", "tf32"])
+def test_axis_tile_heights_agree(shape, precision):
+    """The axis pass has two tile heights (128 image rows, one CTA per SM; 64
+    rows, two CTAs per SM), chosen per shape by timing both on the call's own
+    data.  Both issue the same MMAs for every output element (same K chunks in
+    the same order), so the tuned context returns exactly what a context held
+    at the default height returns."""
+    import ctypes as C
+
+    from wassersteindictionarylearning_b200._lib import check, lib
+    W, H, D = shape
+    N = W * H * D
+    u = np.random.default_rng(11).random(6 * N)
+    tuned = _kern(5.0, W, H, D, precision)
+    plain = _kern(5.0, W, H, D, precision)
+    check(lib().wdl_set_profiling(plain.ctx, 1), plain.ctx)  # profiling keeps the default height
+    first = tuned.convolve(u, 6)   # times both heights
+    again = tuned.convolve(u, 6)   # the chosen height
+    ref = plain.convolve(u, 6)
+    assert np.array_equal(first, ref) and np.array_equal(again, ref)
+    n = lib().wdl_autotune_count(tuned.ctx)
+    key, choice, ms = (C.c_longlong * 6)(), C.c_int(), C.c_float()
+    heights = []
+    for i in range(n):
+        check(lib().wdl_autotune_entry(tuned.ctx, i, key, C.byref(choice), C.byref(ms)), tuned.ctx)
+        if key[0] == 2:
+            assert choice.value in (64, 128) and ms.value > 0
+            heights.append(choice.value)
+    assert len(heights) == (2 if D == 1 else 3)  # one entry per axis-pass shape
+    assert lib().wdl_autotune_count(plain.ctx) == 0
+    tuned.close()
+    plain.close()

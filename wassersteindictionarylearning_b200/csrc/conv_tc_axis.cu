@@ -6,19 +6,25 @@
 // Applying it once per axis returns the image to its layout, as the reference's
 // x-pass into a transposed temporary followed by the y-pass (and z-pass).
 //
-// Each CTA computes a 128 (c) x 128 (r) output tile of one image as a GEMM with
-// M = 128 TMEM lanes = c, N = 128 columns = r, K = C in chunks of 64: A = the
+// Each CTA computes a 128 (c) x TR (r) output tile of one image as a GEMM with
+// M = 128 TMEM lanes = c, N = TR columns = r, K = C in chunks of 64: A = the
 // factor rows c0.., B = the image rows r0.., both K-major in SMEM (128-byte
-// swizzle), in one of two stages while the tensor cores work on the other.  The
+// swizzle), in one of two stages while the tensor cores work on the other.
+// TR = 128 runs one CTA per SM (129 KB of SMEM); TR = 64 halves the image
+// operand (97 KB) so two CTAs share an SM and hide each other's load latency,
+// and splits the launch into twice as many, smaller tiles.  The tile height is
+// chosen per shape by timing both on the call's own data.  The
 // factor is prepared once per context as ready-made operand blocks (split into
 // BF16 hi + lo, or rounded to TF32, already in the swizzled layout), so its
 // blocks are plain 16-byte cp.async copies; the image rows are converted from
 // FP32 by the CTA's threads.  The accumulator row of lane c holds
-// out[c][r0..r0+127], so each thread's epilogue stores are 64-byte contiguous
+// out[c][r0..r0+TR-1], so each thread's epilogue stores are 64-byte contiguous
 // runs of one output row.
 //
 // Precision as the 128-tile operator: kind::tf32, or split BF16 with
 // hi*hi + hi*lo + lo*hi accumulated in FP32 (kind::f16).
+#include <cstring>
+
 #include "tc_common.cuh"
 
 namespace wdl {
@@ -27,14 +33,33 @@ namespace {
 using namespace tc;
 
 constexpr int kAxKc = 64;                  // K elements per chunk
-constexpr int kAxTile = 128;               // output tile: 128 c x 128 r
+constexpr int kAxTile = 128;               // output tile: 128 c x TR r
 constexpr size_t kAxOperand = 32 * 1024;   // one 128 x 64 operand (both BF16 planes / TF32)
-constexpr size_t kAxStage = 2 * kAxOperand;  // A + B
 constexpr int kAxThreads = 256;
 
-// 16-byte chunk (8 BF16 hi + 8 lo, or 4 TF32) of row r, elements k0.. of a
-// 128 x 64 operand whose BF16 lo plane starts 16 KB after the hi plane.
-template <bool SPLIT>
+// Image operand of TR rows x 64 K elements: 128-byte column blocks of TR rows
+// (TR * 128 bytes); two blocks (BF16 hi + lo planes, or TF32 K 0-31 / 32-63).
+template <int TR>
+struct AxGeom {
+  static constexpr uint32_t kRegB = TR * 128;
+  static constexpr size_t kBBytes = 2 * (size_t)kRegB;
+  static constexpr size_t kStage = kAxOperand + kBBytes;  // A + B
+  static constexpr size_t kSmem = 2 * kStage + 1024 + 64;
+};
+
+// Byte offset of element (r, k) in an operand whose 128-byte column blocks
+// are REG bytes apart (the canonical 128-byte swizzle inside each block).
+__device__ __forceinline__ uint32_t swz_reg(int r, int k, int esz, uint32_t reg) {
+  const int per = 128 / esz;
+  const int region = k / per;
+  const int byte = (k - region * per) * esz;
+  const int chunk = (byte >> 4) ^ (r & 7);
+  return (uint32_t)(region * reg + r * 128 + (chunk << 4) + (byte & 15));
+}
+
+// 16-byte chunk (8 BF16 hi + 8 lo, or 4 TF32) of row r, elements k0.. of an
+// operand whose BF16 lo plane starts REG bytes after the hi plane.
+template <bool SPLIT, uint32_t REG>
 __device__ __forceinline__ void put_axis_chunk(uint8_t* tile, int r, int k0, const float* v) {
   if (SPLIT) {
     uint32_t hi[4], lo[4];
@@ -46,11 +71,11 @@ __device__ __forceinline__ void put_axis_chunk(uint8_t* tile, int r, int k0, con
       hi[q] = *reinterpret_cast<const uint32_t*>(&h);
       lo[q] = *reinterpret_cast<const uint32_t*>(&l);
     }
-    const uint32_t o = swz(r, k0, 2);
+    const uint32_t o = swz_reg(r, k0, 2, REG);
     *reinterpret_cast<uint4*>(tile + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    *reinterpret_cast<uint4*>(tile + kRegionBytes + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    *reinterpret_cast<uint4*>(tile + REG + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
   } else {
-    *reinterpret_cast<uint4*>(tile + swz(r, k0, 4)) =
+    *reinterpret_cast<uint4*>(tile + swz_reg(r, k0, 4, REG)) =
         make_uint4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
   }
 }
@@ -60,18 +85,18 @@ __device__ __forceinline__ void put_axis_chunk(uint8_t* tile, int r, int k0, con
 // load_operand, converted and stored into a 128 x 64 operand by
 // store_operand, so the loads of the next chunk can be in flight while the
 // current one is converted and multiplied.
-template <bool SPLIT>
+template <bool SPLIT, int TR>
 struct OperandRegs {
   static constexpr int CE = SPLIT ? 8 : 4;
-  static constexpr int CPR = kAxKc / CE;                 // chunks per row
-  static constexpr int PER = kAxTile * CPR / kAxThreads;  // chunks per thread
+  static constexpr int CPR = kAxKc / CE;            // chunks per row
+  static constexpr int PER = TR * CPR / kAxThreads;  // chunks per thread
   float v[PER][CE];
 };
 
-template <bool SPLIT>
-__device__ __forceinline__ void load_operand(OperandRegs<SPLIT>& o, const float* __restrict__ src, int rows,
+template <bool SPLIT, int TR>
+__device__ __forceinline__ void load_operand(OperandRegs<SPLIT, TR>& o, const float* __restrict__ src, int rows,
                                              int len, int kb, bool vec, int t) {
-  using O = OperandRegs<SPLIT>;
+  using O = OperandRegs<SPLIT, TR>;
 #pragma unroll
   for (int u = 0; u < O::PER; ++u) {
     const int c = t + u * kAxThreads;
@@ -90,14 +115,14 @@ __device__ __forceinline__ void load_operand(OperandRegs<SPLIT>& o, const float*
   }
 }
 
-template <bool SPLIT>
-__device__ __forceinline__ void store_operand(uint8_t* tile, const OperandRegs<SPLIT>& o, int t) {
-  using O = OperandRegs<SPLIT>;
+template <bool SPLIT, int TR>
+__device__ __forceinline__ void store_operand(uint8_t* tile, const OperandRegs<SPLIT, TR>& o, int t) {
+  using O = OperandRegs<SPLIT, TR>;
 #pragma unroll
   for (int u = 0; u < O::PER; ++u) {
     const int c = t + u * kAxThreads;
     const int r = c / O::CPR, kk = (c - r * O::CPR) * O::CE;
-    put_axis_chunk<SPLIT>(tile, r, kk, o.v[u]);
+    put_axis_chunk<SPLIT, AxGeom<TR>::kRegB>(tile, r, kk, o.v[u]);
   }
 }
 
@@ -124,25 +149,26 @@ __global__ void k_build_factor_blocks(const float* __restrict__ G, int C, uint8_
       const int row = c0 + r, k = j * kAxKc + kk + q;
       v[q] = (row < C && k < C) ? G[(size_t)row * C + k] : 0.f;
     }
-    put_axis_chunk<SPLIT>(tile, r, kk, v);
+    put_axis_chunk<SPLIT, kRegionBytes>(tile, r, kk, v);
   }
 }
 
-template <bool SPLIT>
-__global__ void __launch_bounds__(kAxThreads, 1)
+template <bool SPLIT, int TR>
+__global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
     tc_axis_kernel(const float* __restrict__ in, float* __restrict__ out,
                    const uint8_t* __restrict__ gblocks, int R, int C, size_t img_stride, int* err) {
+  using Ge = AxGeom<TR>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 2 * kAxStage);  // [2]
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + 2 * kAxStage + 16);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 2 * Ge::kStage);  // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + 2 * Ge::kStage + 16);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int c0 = blockIdx.x * kAxTile, r0 = blockIdx.y * kAxTile;
+  const int c0 = blockIdx.x * kAxTile, r0 = blockIdx.y * TR;
   const float* src = in + (size_t)blockIdx.z * img_stride + (size_t)r0 * C;
   const int nch = (C + kAxKc - 1) / kAxKc;
   const uint8_t* gsrc = gblocks + (size_t)blockIdx.x * nch * kAxOperand;
   float* dst = out + (size_t)blockIdx.z * img_stride;
-  const int b_rows = min(kAxTile, R - r0);
+  const int b_rows = min(TR, R - r0);
   const bool vec = (C & 3) == 0;
 
   if (t == 0) {
@@ -150,20 +176,20 @@ __global__ void __launch_bounds__(kAxThreads, 1)
     ptx::mbar_init(ptx::smem_addr(&bars[1]), 1);
     ptx::fence_mbar_init();
   }
-  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tslot), 128);
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tslot), TR);
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t d = *tslot;
 
   using F = Fmt<SPLIT>;
-  const uint32_t id = ptx::idesc(F::fmt, 128, 128);
+  const uint32_t id = ptx::idesc(F::fmt, 128, TR);
   bool ok = true;
-  OperandRegs<SPLIT> breg;
-  load_operand<SPLIT>(breg, src, b_rows, C, 0, vec, t);
+  OperandRegs<SPLIT, TR> breg;
+  load_operand<SPLIT, TR>(breg, src, b_rows, C, 0, vec, t);
   for (int j = 0; j < nch; ++j) {
     const int st = j & 1;
-    uint8_t* a_tile = base + st * kAxStage;
+    uint8_t* a_tile = base + st * Ge::kStage;
     uint8_t* b_tile = a_tile + kAxOperand;
     if (j >= 2) {  // the MMAs of chunk j-2 read this stage: wait for their commit
       const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[st]), (uint32_t)(((j - 2) >> 1) & 1), kWaitNs);
@@ -180,8 +206,8 @@ __global__ void __launch_bounds__(kAxThreads, 1)
       }
       cp_async_commit();
     }
-    store_operand<SPLIT>(b_tile, breg, t);
-    if (j + 1 < nch) load_operand<SPLIT>(breg, src, b_rows, C, (j + 1) * kAxKc, vec, t);
+    store_operand<SPLIT, TR>(b_tile, breg, t);
+    if (j + 1 < nch) load_operand<SPLIT, TR>(breg, src, b_rows, C, (j + 1) * kAxKc, vec, t);
     cp_async_wait_all();
     ptx::fence_proxy_async_smem();
     ptx::tc_fence_before();
@@ -193,12 +219,13 @@ __global__ void __launch_bounds__(kAxThreads, 1)
 #pragma unroll
       for (int ks = 0; ks < steps; ++ks) {
         const uint32_t byte = (uint32_t)ks * 32u;
-        const uint32_t off = (byte >> 7) * kRegionBytes + (byte & 127u);
+        const uint32_t offa = (byte >> 7) * kRegionBytes + (byte & 127u);
+        const uint32_t offb = (byte >> 7) * Ge::kRegB + (byte & 127u);
         const uint32_t acc = (j > 0 || ks > 0) ? 1u : 0u;
-        const uint64_t ad = ptx::sw128_desc(a + off), bd = ptx::sw128_desc(b + off);
+        const uint64_t ad = ptx::sw128_desc(a + offa), bd = ptx::sw128_desc(b + offb);
         if (SPLIT) {
-          const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + off);
-          const uint64_t blo = ptx::sw128_desc(b + kRegionBytes + off);
+          const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + offa);
+          const uint64_t blo = ptx::sw128_desc(b + Ge::kRegB + offb);
           ptx::mma_bf16(d, ad, bd, id, acc);
           ptx::mma_bf16(d, ad, blo, id, 1u);
           ptx::mma_bf16(d, alo, bd, id, 1u);
@@ -222,9 +249,9 @@ __global__ void __launch_bounds__(kAxThreads, 1)
     const int c = c0 + q * 32 + lane;
     const bool rvec = (R & 3) == 0;
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc) {
+    for (int cc = 0; cc < TR / 32; ++cc) {
       float v[16];
-      const int col = half * 64 + cc * 16;
+      const int col = half * (TR / 2) + cc * 16;
       ptx::tmem_ld16(d + ((uint32_t)(q * 32) << 16) + (uint32_t)col, v);
       ptx::tmem_ld_wait();
       if (c < C) {
@@ -246,27 +273,80 @@ __global__ void __launch_bounds__(kAxThreads, 1)
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
-  if (warp == 0) ptx::tmem_dealloc(d, 128);
+  if (warp == 0) ptx::tmem_dealloc(d, TR);
 }
 
-size_t axis_smem() { return 2 * kAxStage + 1024 + 64; }
-
-int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
-                 size_t img_stride, int* err, cudaStream_t s) {
+template <int TR>
+int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
+                   size_t img_stride, int* err, cudaStream_t s) {
   size_t done = 0;
   while (done < nimg) {
     size_t chunk = nimg - done;
     if (chunk > 65535) chunk = 65535;
-    dim3 grid((C + kAxTile - 1) / kAxTile, (R + kAxTile - 1) / kAxTile, (unsigned)chunk);
+    dim3 grid((C + kAxTile - 1) / kAxTile, (R + TR - 1) / TR, (unsigned)chunk);
+    const size_t smem = AxGeom<TR>::kSmem;
     if (ctx->precision == WDL_SPLIT_BF16)
-      tc_axis_kernel<true><<<grid, kAxThreads, axis_smem(), s>>>(in + done * img_stride, out + done * img_stride,
-                                                                 G, R, C, img_stride, err);
+      tc_axis_kernel<true, TR><<<grid, kAxThreads, smem, s>>>(in + done * img_stride, out + done * img_stride,
+                                                              G, R, C, img_stride, err);
     else
-      tc_axis_kernel<false><<<grid, kAxThreads, axis_smem(), s>>>(in + done * img_stride, out + done * img_stride,
-                                                                  G, R, C, img_stride, err);
+      tc_axis_kernel<false, TR><<<grid, kAxThreads, smem, s>>>(in + done * img_stride, out + done * img_stride,
+                                                               G, R, C, img_stride, err);
     WDL_LAUNCH_CHECK(ctx);
     done += chunk;
   }
+  return WDL_OK;
+}
+
+int tc_axis_dispatch(wdl_ctx* ctx, int TR, const float* in, float* out, const uint8_t* G, int R, int C,
+                     size_t nimg, size_t img_stride, int* err, cudaStream_t s) {
+  return TR == 64 ? tc_axis_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, err, s)
+                  : tc_axis_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, err, s);
+}
+
+// Tile height per shape (rows, row length, image count, precision): the first
+// call of a shape outside a graph capture and outside profiling runs both
+// heights on the call's own data (once untimed, once timed with CUDA events on
+// the call's stream) and keeps the faster; WDL_AUTOTUNE=0 keeps 128.  Both
+// heights issue the same MMAs for every output element (same K chunks, same
+// order), so the choice does not change results.
+int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
+                 size_t img_stride, int* err, cudaStream_t s) {
+  const long long key[6] = {2, R, C, (long long)nimg, ctx->precision == WDL_SPLIT_BF16 ? 2 : 4, 0};
+  for (const auto& e : ctx->tuned)
+    if (!std::memcmp(e.key, key, sizeof(key)))
+      return tc_axis_dispatch(ctx, e.choice, in, out, G, R, C, nimg, img_stride, err, s);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  if (!autotune_enabled() || cap != cudaStreamCaptureStatusNone || ctx->profiling)
+    return tc_axis_dispatch(ctx, 128, in, out, G, R, C, nimg, img_stride, err, s);
+  const int cand[2] = {128, 64};
+  int best = 128;
+  float best_ms = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WDL_CUDA_TRY(ctx, cudaEventCreate(&e0));
+  WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
+  int rc = WDL_OK;
+  for (int c : cand) {
+    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, err, s))) break;
+    cudaEventRecord(e0, s);
+    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, err, s))) break;
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  wdl_ctx::TuneEntry te;
+  std::memcpy(te.key, key, sizeof(key));
+  te.choice = best;
+  te.ms = best_ms;
+  ctx->tuned.push_back(te);
   return WDL_OK;
 }
 
@@ -280,10 +360,14 @@ size_t factor_block_bytes(int C) {
 // Sets the kernels' SMEM limit and builds the factor blocks of every axis
 // (blocks[a], at most 4 x 8 x 32 KB = 1 MB per axis for sides up to 512).
 int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]) {
-  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)axis_smem()));
-  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)axis_smem()));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxGeom<128>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxGeom<128>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxGeom<64>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxGeom<64>::kSmem));
   const bool split = ctx->precision == WDL_SPLIT_BF16;
   for (int a = 0; a < ctx->ndim; ++a) {
     const int C = ctx->axis_len[a];
