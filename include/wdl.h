@@ -254,8 +254,14 @@ int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launch
                      double* conv_images);
 /* Launch shapes the autotuner chose on this context: entry i has key {kind,
  * rows, row length, images, element bytes, signed} (kind 1 = log-domain axis
- * pass), the chosen variant (rows per block) and its time in ms.
- * wdl_autotune_count returns the number of entries. */
+ * pass: variant = rows per block; kind 2 = tensor-core axis pass: variant =
+ * output tile height, element bytes 2 for split BF16 and 4 for TF32), the
+ * chosen variant and its time in ms.  wdl_autotune_count returns the number of
+ * entries.  wdl_set_autotune(ctx, 0) stops this context from timing variants
+ * on first calls (a latency-bound caller such as a request loop, where every
+ * timing would also synchronise the stream); untuned shapes then take the
+ * default variant.  On by default; WDL_AUTOTUNE=0 turns it off process-wide. */
+int wdl_set_autotune(wdl_ctx* ctx, int on);
 int wdl_autotune_count(const wdl_ctx* ctx);
 int wdl_autotune_entry(const wdl_ctx* ctx, int i, long long* key6, int* choice, float* ms);
 /* Exponentials the log-domain operator evaluated while profiling (the

@@ -68,9 +68,10 @@ def test_uneven_weight_fitting(oracle):
     from wassersteindictionarylearning_b200.batch import fit_weights, uneven_problems
     probs = uneven_problems(n=12, seed=3, sides=(32, 48, 64, 144), K_range=(3, 5), L_range=(6, 12),
                             gammas=(1.0, 2.0))
-    res = fit_weights(probs, precision="split_bf16", lbfgs_iterations=8)
+    res = fit_weights(probs, precision="split_bf16", lbfgs_iterations=8, epsilon=1e-6)
     # the peaked atoms at gamma 2 overflow the FP32 kernel-domain scalings
     # within these iteration counts: those problems finish in the log domain
+    # (a gradient test of 1e-6 lets the fits that stay in range stop early)
     assert {r[4] for r in res} == {"kernel", "log"}
     for pr, (w, f, status, evals, domain) in zip(probs, res):
         assert np.isfinite(f) and evals >= 2

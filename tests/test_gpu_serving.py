@@ -19,9 +19,9 @@ def _stream(n, seed, sides=(32, 48, 64), frac_3d=0.2, cube=12, rate=400.0):
     return poisson_requests(rate, n, seed=seed, K=3, frac_3d=frac_3d, sides=sides, cube=cube)
 
 
-def _engine(precision, **kw):
+def _engine(precision, gamma=2.0, **kw):
     from wassersteindictionarylearning_b200.serving import ServingEngine
-    return ServingEngine(K=3, L=12, gamma=2.0, loss_type=2, precision=precision,
+    return ServingEngine(K=3, L=12, gamma=gamma, loss_type=2, precision=precision,
                          lbfgs_iterations=8, **kw)
 
 
@@ -69,16 +69,49 @@ def test_admission_by_bytes():
     big = Request(PROJECTION, (64, 64, 1), observed=blob_histograms(1, 64, 64, seed=1)[0])
     small = [Request(PROJECTION, (32, 32, 1), observed=blob_histograms(1, 32, 32, seed=2 + i)[0])
              for i in range(3)]
-    probe = _engine("fp32")
+    # gamma 8: the FP32 scalings stay in range, so no request moves to FP64
+    probe = _engine("fp32", gamma=8.0)
     b_small, b_big = probe.request_bytes(small[0]), probe.request_bytes(big)
     probe.close()
     assert b_big > 1.6 * b_small
-    eng = _engine("fp32", hbm_budget=1.5 * b_small)  # room for one small request at a time
+    eng = _engine("fp32", gamma=8.0, hbm_budget=1.5 * b_small)  # room for one small request at a time
     done = eng.run([(0.0, big)] + [(0.0, s) for s in small])
     st = {r.rid: r.status for r in done}
     assert st[0] == -7                       # WDL_ERR_ADMISSION: never fits
     assert all(st[i] == 0 for i in (1, 2, 3))  # served one after another
     order = [r.rid for r in done if r.status == 0]
     assert order == [1, 2, 3]
-    assert eng.admitted_bytes == 0
+    assert eng.admitted_bytes == 0 and not eng.wide_shapes
     eng.close()
+
+
+def test_fp32_overflow_is_served_in_fp64():
+    """Blob dictionary, gamma 2, L 50 on a 64 x 64 grid: the kernel-domain
+    scalings pass 1e60, beyond FP32 and inside FP64.  The split-BF16 engine's
+    requests start over on the shape's FP64 context, so they return exactly
+    what an FP64 engine returns; start-up calibration finds the shape too."""
+    import copy
+
+    from wassersteindictionarylearning_b200.serving import (BARYCENTER, PROJECTION, Request,
+                                                            ServingEngine)
+    from wassersteindictionarylearning_b200.synthetic import blob_histograms
+    shape = (64, 64, 1)
+    reqs = [(0.0, Request(PROJECTION, shape, observed=blob_histograms(1, 64, 64, seed=9)[0])),
+            (0.0, Request(BARYCENTER, shape, weights=np.array([0.1, 0.2, 0.3, 0.25, 0.15])))]
+
+    def mk(precision):
+        return ServingEngine(K=5, L=50, gamma=2.0, loss_type=2, precision=precision,
+                             lbfgs_iterations=4)
+    eng, ref = mk("split_bf16"), mk("fp64")
+    got = sorted(eng.run(copy.deepcopy(reqs)), key=lambda r: r.rid)
+    want = sorted(ref.run(copy.deepcopy(reqs)), key=lambda r: r.rid)
+    assert shape in eng.wide_shapes
+    for g, w in zip(got, want):
+        assert g.status == 0 and g.form == "fp64" and np.all(np.isfinite(g.result))
+        assert np.array_equal(g.result, w.result), g.kind
+    eng.close()
+    ref.close()
+    cal = mk("split_bf16")
+    cal.preload([shape])
+    assert shape in cal.wide_shapes
+    cal.close()

@@ -96,6 +96,7 @@ SIGNATURES = {
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),
     "wdl_phase_trace": ([_vp, _dp], C.c_int),
     "wdl_exp_profile": ([_vp, _dp], C.c_int),
+    "wdl_set_autotune": ([_vp, C.c_int], C.c_int),
     "wdl_autotune_count": ([_vp], C.c_int),
     "wdl_autotune_entry": ([_vp, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                             C.POINTER(C.c_float)], C.c_int),

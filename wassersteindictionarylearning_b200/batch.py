@@ -65,13 +65,16 @@ def batch_run(kernel, problems):
     return outs
 
 
-def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6, log_domain=False):
+def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-50, log_domain=False):
     """wdl_fit_weights: every histogram of every problem fitted by its own
     L-BFGS on the device, all evaluated together each round.  problems: dicts
     with W, H, K, L, atoms [K*N], observed [P*N] (P = len / N), loss_type,
     optional x0 [P*K].  Returns per problem (weights [P,K], loss [P], status
     [P], evaluations [P]).  log_domain: wdl_fit_weights_log on a log-domain
-    kernel (one persistent launch, each fit wholly on the device)."""
+    kernel (one persistent launch, each fit wholly on the device).  epsilon:
+    the L-BFGS gradient test; the default 1e-50 is regress_both's setting
+    (cpp/inverseWasserstein.h:366), so every fit runs its full iteration
+    budget unless its line search stops it."""
     n = len(problems)
     arr = (WdlFitProblem * n)()
     keep, outs = [], []
@@ -95,7 +98,7 @@ def fit_device(kernel, problems, lbfgs_iterations=40, epsilon=1e-6, log_domain=F
 
 
 def fit_weights(problems, precision="split_bf16", lbfgs_iterations=40, device=0, max_side=128,
-                epsilon=1e-6):
+                epsilon=1e-50):
     """problems: dicts with W, H, K, L, gamma, atoms [K*N], observed [N],
     loss_type.  Returns per problem (weights [K], loss, lbfgs status,
     evaluations, domain).

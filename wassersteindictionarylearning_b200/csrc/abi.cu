@@ -303,6 +303,12 @@ int wdl_phase_trace(wdl_ctx* ctx, double* out27) {
   return WDL_OK;
 }
 
+int wdl_set_autotune(wdl_ctx* ctx, int on) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  ctx->autotune = on != 0;
+  return WDL_OK;
+}
+
 int wdl_autotune_count(const wdl_ctx* ctx) { return ctx ? (int)ctx->tuned.size() : WDL_ERR_INVALID_ARG; }
 
 int wdl_autotune_entry(const wdl_ctx* ctx, int i, long long* key6, int* choice, float* ms) {

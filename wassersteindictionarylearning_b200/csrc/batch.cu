@@ -155,7 +155,7 @@ int batch_prepare(wdl_ctx* ctx, const wdl_problem* pb, int nprob, size_t extra_b
       o.lam = c.take<float>(P * K);
       o.cb = c.take<float>(fo ? 1 : slots * P * K * N);
       o.phi = c.take<float>(slots * P * K * N);
-      o.sync = c.take<int>(4 * P);
+      o.sync = c.take<int>(5 * P);
     }
     bp.in_b = c.mark();  // inputs: one upload
     for (int q = 0; q < nprob; ++q) {

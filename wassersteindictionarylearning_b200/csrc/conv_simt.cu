@@ -310,7 +310,7 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
       return log_axis_dispatch<T>(ctx, e.choice, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
-  if (!autotune_enabled() || cap != cudaStreamCaptureStatusNone || ctx->profiling)
+  if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
     return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
   const int cand[3] = {8, 16, 32};
   int best = kLogRowsDefault;

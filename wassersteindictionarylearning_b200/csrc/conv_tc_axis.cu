@@ -303,12 +303,20 @@ int tc_axis_dispatch(wdl_ctx* ctx, int TR, const float* in, float* out, const ui
                   : tc_axis_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, err, s);
 }
 
+// Default tile height: 64 while the 128-row grid would fill fewer than two
+// waves of one CTA per SM (more, smaller tiles, two per SM), else 128.
+int tc_axis_default_height(const wdl_ctx* ctx, int R, int C, size_t nimg) {
+  const size_t tiles128 = (size_t)((C + kAxTile - 1) / kAxTile) * (size_t)((R + kAxTile - 1) / kAxTile) * nimg;
+  return tiles128 < 2 * (size_t)ctx->sm_count ? 64 : 128;
+}
+
 // Tile height per shape (rows, row length, image count, precision): the first
 // call of a shape outside a graph capture and outside profiling runs both
 // heights on the call's own data (once untimed, once timed with CUDA events on
-// the call's stream) and keeps the faster; WDL_AUTOTUNE=0 keeps 128.  Both
-// heights issue the same MMAs for every output element (same K chunks, same
-// order), so the choice does not change results.
+// the call's stream) and keeps the faster; with autotuning off (WDL_AUTOTUNE=0,
+// wdl_set_autotune) the default height is taken.  Both heights issue the same
+// MMAs for every output element (same K chunks, same order), so the choice
+// does not change results.
 int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
                  size_t img_stride, int* err, cudaStream_t s) {
   const long long key[6] = {2, R, C, (long long)nimg, ctx->precision == WDL_SPLIT_BF16 ? 2 : 4, 0};
@@ -317,10 +325,11 @@ int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, in
       return tc_axis_dispatch(ctx, e.choice, in, out, G, R, C, nimg, img_stride, err, s);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
-  if (!autotune_enabled() || cap != cudaStreamCaptureStatusNone || ctx->profiling)
-    return tc_axis_dispatch(ctx, 128, in, out, G, R, C, nimg, img_stride, err, s);
+  const int dflt = tc_axis_default_height(ctx, R, C, nimg);
+  if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
+    return tc_axis_dispatch(ctx, dflt, in, out, G, R, C, nimg, img_stride, err, s);
   const int cand[2] = {128, 64};
-  int best = 128;
+  int best = dflt;
   float best_ms = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e0));

@@ -132,17 +132,33 @@ __global__ void k_normalise_rows(const double* __restrict__ in, double* __restri
 }
 
 // ---------------- kernel-domain forward (cpp/inverseWasserstein.h:565-593) -----------
+// Out-of-range scalings: with a narrow kernel the kernel-domain scalings grow
+// with the iterations (past 1e60 within 50 iterations at gamma = 2 px^2 for
+// dictionaries with empty regions), beyond the FP32 range where the reference's
+// FP64 still holds them.  In FP32 a scaling then saturates (inf, or a 0 that
+// turns the next ratio into inf or NaN), and later iterations can carry on with
+// finite but meaningless values.  The FP32 forms record per histogram whether
+// a scaling a or b was ever non-finite (range[p], when given), and such a
+// histogram's barycenter is replaced by NaN after the forward pass, so its
+// loss and gradients report the overflow as NaN, as the FP64 path would
+// report one of its own.
+
 // a = p / conv_b, the atoms shared by every histogram.
 template <typename T>
 __global__ void k_div_atoms(const T* __restrict__ atoms, const T* __restrict__ cb,
-                            T* __restrict__ a, size_t KN, size_t total) {
-  GRID_STRIDE(i, total) a[i] = atoms[i % KN] / cb[i];
+                            T* __restrict__ a, size_t KN, size_t total, int* __restrict__ range) {
+  GRID_STRIDE(i, total) {
+    const T v = atoms[i % KN] / cb[i];
+    a[i] = v;
+    if (range && !isfinite(v)) range[i / KN] = 1;
+  }
 }
 
 // Weighted geometric mean over the K atoms and the next scalings b = bary / phi.
 template <typename T>
 __global__ void k_bary_b(const T* __restrict__ phi, const double* __restrict__ lam,
-                         T* __restrict__ b, T* __restrict__ bary, int K, size_t N, size_t PN) {
+                         T* __restrict__ b, T* __restrict__ bary, int K, size_t N, size_t PN,
+                         int* __restrict__ range) {
   GRID_STRIDE(idx, PN) {
     const size_t p = idx / N, j = idx - p * N;
     const T* ph = phi + p * K * N + j;
@@ -150,9 +166,23 @@ __global__ void k_bary_b(const T* __restrict__ phi, const double* __restrict__ l
     for (int k = 0; k < K; ++k) s += acc_safe_log<T>(ph[k * N]) * lam[p * K + k];
     const T by = exp_from<T>(s);
     bary[idx] = by;
-    if (b)
-      for (int k = 0; k < K; ++k) b[p * K * N + k * N + j] = by / ph[k * N];
+    if (b) {
+      bool bad = false;
+      for (int k = 0; k < K; ++k) {
+        const T bv = by / ph[k * N];
+        b[p * K * N + k * N + j] = bv;
+        bad |= !isfinite(bv);
+      }
+      if (range && bad) range[p] = 1;
+    }
   }
+}
+
+// NaN barycenters for the histograms whose scalings left the range.
+template <typename T>
+__global__ void k_poison_out_of_range(T* __restrict__ bary, const int* __restrict__ range, size_t N,
+                                      size_t PN) {
+  GRID_STRIDE(idx, PN) if (range[idx / N]) bary[idx] = T(NAN);
 }
 
 // ---------------- log-domain forward (:700-720, :167-196) ---------------------------
@@ -476,6 +506,7 @@ struct EvalBufs {
   T *atoms, *lam, *tape_b, *tape_cb, *tape_phi, *a, *bary, *n, *gw, *buf2, *cbuf2, *v, *r, *ctmp;
   T *wa = nullptr, *wb = nullptr, *wc = nullptr, *wgrad = nullptr;
   double *atoms64, *lam64, *gdic, *dot, *loss, *dpart;
+  int* range;  // [P] scalings left the FP32 range (kernel domain, FP32 forms)
   uint8_t *sd = nullptr, *sw = nullptr, *stmp = nullptr;
 
   template <class A>
@@ -503,6 +534,7 @@ struct EvalBufs {
     d(dot, P * K);
     d(dpart, P * K * n_segments(N));
     d(loss, P);
+    alloc_into(al, reinterpret_cast<void**>(&range), P * sizeof(int));
     if (wloss) {
       t(wa, PN);
       t(wb, PN);
@@ -590,6 +622,8 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
   WDL_LAUNCH_CHECK(ctx);
 
   // Forward Bregman projections, storing b, conv_b and phi (:565-593 / :700-720).
+  int* range = (!log_domain && sizeof(T) == 4) ? B.range : nullptr;
+  if (range) WDL_CUDA_TRY(ctx, cudaMemsetAsync(range, 0, (size_t)P * sizeof(int), s));
   for (int it = 1; it <= L; ++it) {
     const T* b_prev = B.tape_b + (size_t)(it - 1) * PKN;
     T* cb = B.tape_cb + (size_t)(it - 1) * PKN;
@@ -597,10 +631,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
     T* b_next = B.tape_b + (size_t)it * PKN;
     if (!log_domain) {
       if ((rc = conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, s))) return rc;
-      k_div_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN);
+      k_div_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN, range);
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, s))) return rc;
-      k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam64, b_next, B.bary, K, N, PN);
+      k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam64, b_next, B.bary, K, N, PN, range);
     } else {
       if ((rc = log_conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, nullptr, nullptr,
                                   nullptr, s)))
@@ -616,6 +650,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
   }
   if (log_domain) {
     k_exp_inplace<T><<<G_PN, 256, 0, s>>>(B.bary, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
+  if (range) {
+    k_poison_out_of_range<T><<<G_PN, 256, 0, s>>>(B.bary, range, N, PN);
     WDL_LAUNCH_CHECK(ctx);
   }
 
@@ -714,6 +752,8 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
   T* a = A.take<T>(PKN);
   T* tmp = A.take<T>(PKN);
   T* bary = A.take<T>(PN);
+  int* range = (!log_domain && sizeof(T) == 4) ? A.take<int>((size_t)P) : nullptr;
+  if (range) WDL_CUDA_TRY(ctx, cudaMemsetAsync(range, 0, (size_t)P * sizeof(int), s));
   k_normalise_rows<<<K, 256, 0, s>>>(atoms, atoms64, N, 0.0);
   WDL_LAUNCH_CHECK(ctx);
   k_normalise_rows<<<P, 32, 0, s>>>(weights, lam64, K, 0.0);
@@ -728,10 +768,10 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
   for (int it = 0; it < L; ++it) {
     if (!log_domain) {
       if ((rc = conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, s))) return rc;
-      k_div_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN);
+      k_div_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN, range);
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, s))) return rc;
-      k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam64, b, bary, K, N, PN);
+      k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam64, b, bary, K, N, PN, range);
     } else {
       if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
         return rc;
@@ -747,6 +787,10 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
     k_exp_inplace<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(bary, PN);
     WDL_LAUNCH_CHECK(ctx);
   }
+  if (range) {
+    k_poison_out_of_range<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(bary, range, N, PN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
   k_cast_back<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(bary, bary_out, PN);
   WDL_LAUNCH_CHECK(ctx);
   return WDL_OK;
@@ -757,7 +801,7 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
 struct FusedBufs {
   double *atoms64, *lam64, *dot, *loss;
   float *atoms, *lam, *b0, *cb, *phi, *acc, *nb, *gwb, *v, *r, *gdic;
-  int* sync;       // work, err, then done_fwd/bary_ready/done_bwd/msg_ready [4P]
+  int* sync;       // work, err, then done_fwd/bary_ready/done_bwd/msg_ready/range [5P]
   SkProblem* prob; // device copy of the problem descriptor
   template <class A>
   void layout(A& al, size_t P, size_t K, size_t L, size_t N, bool b_init, bool fwd_only) {
@@ -780,7 +824,7 @@ struct FusedBufs {
     f(v, fwd_only ? 1 : PKN);
     f(r, fwd_only ? 1 : PKN);
     f(gdic, fwd_only ? 1 : PKN);
-    alloc_into(al, reinterpret_cast<void**>(&sync), (2 + 4 * P) * sizeof(int));
+    alloc_into(al, reinterpret_cast<void**>(&sync), (2 + 5 * P) * sizeof(int));
     alloc_into(al, reinterpret_cast<void**>(&prob), sizeof(SkProblem));
   }
 };
@@ -932,7 +976,7 @@ size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K) {
   if (tc_fused(ctx) && ctx->domain == WDL_DOMAIN_KERNEL) return fused_bytes(P, K, 2, ctx->N, false, true);
   const size_t N = ctx->N, KN = (size_t)K * N, PKN = (size_t)P * KN, PN = (size_t)P * N;
   const size_t t = use_fp64(ctx) ? 8 : 4;
-  return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 16 * 256;
+  return 8 * (KN + (size_t)P * K) + t * (KN + (size_t)P * K + 4 * PKN + PN) + 4 * (size_t)P + 17 * 256;
 }
 
 // The CUDA-core path issues ~7 launches per iteration and reverse step (about

@@ -31,6 +31,8 @@
 // column-form result, after the elementwise step, is exactly the row form's
 // K-major operand, so every SMEM write is a whole 16-byte chunk and every
 // global access of the epilogue is a contiguous row segment.
+#include <cfloat>
+
 #include "tc_common.cuh"
 #include "wdl_math.cuh"
 
@@ -439,6 +441,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     int* bary_ready = done_fwd + P;
     int* done_bwd = bary_ready + P;
     int* msg_ready = done_bwd + P;
+    int* range = msg_ready + P;  // a scaling of histogram p left the FP32 range
     // Tape slot of iteration it (1..L): all L kept for the reverse pass; two
     // slots suffice for a forward-only run.
     auto slot = [&](int it) -> size_t { return fwd_only ? (size_t)((it - 1) & 1) : (size_t)(it - 1); };
@@ -490,6 +493,13 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
 
     if (type == 0) {  // ---------------- forward Bregman iteration
       const int it = step;
+      // Scalings beyond the FP32 range (narrow kernels: they grow with the
+      // iterations where FP64 still holds them) saturate to inf or to 0.  Every
+      // such chain reaches phi = conv(a) as 0 (b = bary / phi overflows) or
+      // inf (a = p / conv_b overflows): a histogram whose phi leaves (0, inf)
+      // is flagged, and after the launch its barycenter, loss and gradients
+      // are set to NaN (k_poison_flagged).
+      bool bad = false;
       float* cb_out = pr->cb + slot(it) * PKN + pk * N;
       float* phi_out = pr->phi + slot(it) * PKN + pk * N;
       float* acc_out = pr->acc + slot(it) * PN + (size_t)p * N;
@@ -521,9 +531,12 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       const float* esrc[1] = {nullptr};
       epi_rows_red<0>(c, g, esrc, acc_out, [&](size_t idx, float4 y, const float (&)[1][4], int nv) {
         st4(phi_out + idx, y, nv, g.vec);
+        const float o[4] = {y.x, y.y, y.z, y.w};
+        for (int r = 0; r < nv; ++r) bad |= !(o[r] > 0.f && o[r] <= FLT_MAX);
         return make_float4(lam * safe_logf(y.x), lam * safe_logf(y.y), lam * safe_logf(y.z),
                            lam * safe_logf(y.w));
       });
+      if (bad) *(volatile int*)(range + p) = 1;
       tr.mark(6);
     } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
       const int s = step;
@@ -692,13 +705,40 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   if (warp == 0) ptx::tmem_dealloc(*tmem_slot, 2 * kTmemCols);
 }
 
-// Per-problem sync words: done_fwd, bary_ready (0), done_bwd, msg_ready (-1).
+// Histograms whose forward pass flagged scalings beyond the FP32 range
+// (range[p]): barycenter, loss, weight gradient and their share of the
+// dictionary gradient set to NaN, as an overflow in FP64 would leave them.
+__global__ void k_poison_flagged(const SkProblem* probs, int nprobs) {
+  const float qnan = __int_as_float(0x7fc00000);
+  for (int q = blockIdx.x; q < nprobs; q += gridDim.x) {
+    const SkProblem& pr = probs[q];
+    const int P = pr.P, K = pr.K;
+    const int* range = pr.sync + 4 * P;
+    const size_t N = pr.N, PN = (size_t)P * N;
+    const size_t last = pr.fwd_only ? (size_t)((pr.L - 1) & 1) : (size_t)(pr.L - 1);
+    for (int p = 0; p < P; ++p) {
+      if (!range[p]) continue;
+      float* acc = pr.acc + last * PN + (size_t)p * N;
+      for (size_t j = threadIdx.x; j < N; j += blockDim.x) acc[j] = qnan;
+      if (pr.fwd_only) continue;
+      if (threadIdx.x == 0) pr.loss[p] = (double)qnan;
+      for (int k = threadIdx.x; k < K; k += blockDim.x) pr.dot[(size_t)p * K + k] = (double)qnan;
+      if (pr.need_dic) {
+        float* gd = pr.gdic + (size_t)p * K * N;
+        for (size_t j = threadIdx.x; j < (size_t)K * N; j += blockDim.x) gd[j] = qnan;
+      }
+    }
+  }
+}
+
+// Per-problem sync words: done_fwd, bary_ready (0), done_bwd, msg_ready (-1),
+// range (0).
 __global__ void k_sync_init(int* work_err, const SkProblem* probs, int nprobs) {
   if (blockIdx.x == 0 && threadIdx.x < 2) work_err[threadIdx.x] = 0;
   for (int q = blockIdx.x; q < nprobs; q += gridDim.x) {
     const int P = probs[q].P;
     int* s = probs[q].sync;
-    for (int i = threadIdx.x; i < 4 * P; i += blockDim.x) s[i] = i >= 3 * P ? -1 : 0;
+    for (int i = threadIdx.x; i < 5 * P; i += blockDim.x) s[i] = (i >= 3 * P && i < 4 * P) ? -1 : 0;
   }
 }
 
@@ -750,6 +790,8 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
   if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
   if (split) sinkhorn_tc_kernel<true><<<grid, 2 * kSt, smem, s>>>(a);
   else sinkhorn_tc_kernel<false><<<grid, 2 * kSt, smem, s>>>(a);
+  WDL_LAUNCH_CHECK(ctx);
+  k_poison_flagged<<<a.nprobs < 256 ? a.nprobs : 256, 256, 0, s>>>(a.probs, a.nprobs);
   WDL_LAUNCH_CHECK(ctx);
   if (ctx->profiling) {
     cudaEventRecord(ctx->ev_b, s);

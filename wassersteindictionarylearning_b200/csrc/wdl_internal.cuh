@@ -81,6 +81,7 @@ struct wdl_ctx {
   long long launches = 0;
 
   bool profiling = false;
+  bool autotune = true;  // wdl_set_autotune
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   double conv_ms = 0;
   long long conv_launches = 0;
@@ -222,7 +223,7 @@ struct SkProblem {
   float *v, *r, *gdic;   // [P][K][N]
   double* dot;           // [P][K]
   double* loss;          // [P]
-  int* sync;             // done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P]
+  int* sync;             // done_fwd[P], bary_ready[P], done_bwd[P], msg_ready[P], range[P]
 };
 
 struct SkArgs {
