@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-rates", default="50,200,500,2000")
-    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=120)
     # Reduced sizes for profiler captures (the bench line itself uses the workload's).
     ap.add_argument("--P", type=int, default=None)
     ap.add_argument("--L", type=int, default=None)
@@ -554,8 +554,9 @@ def run_uneven_reference(args):
     domain the workload needs; LogSignArrayGaussian2DKernel, OpenMP over all
     host cores).  Bounded sample: one evaluation of each of the two problems
     of median operator work (K L N (W + H)); the whole workload's time is that
-    rate times the workload's total work, times the 14.9 evaluations per fit
-    our run of the same problems used."""
+    rate times the workload's total work, times the 57.1 evaluations per fit
+    our run of the same problems used (regress_both's L-BFGS settings: each fit
+    runs its 40 iterations unless the line search stops it)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -581,7 +582,7 @@ def run_uneven_reference(args):
                           log_domain=True)
         t_sample += time.perf_counter() - t0
         w_sample += work[i]
-    evals_per_fit = 14.9
+    evals_per_fit = 57.1
     total = sum(work) / w_sample * t_sample * evals_per_fit
     value = len(probs) / total
     desc = ", ".join(f"{probs[i]['W']}x{probs[i]['H']} K={probs[i]['K']} L={probs[i]['L']}" for i in sample)
