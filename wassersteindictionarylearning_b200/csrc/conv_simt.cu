@@ -16,17 +16,31 @@ namespace wdl {
 namespace {
 
 // ---- dense axis pass: out[c][r] = sum_k in[r][k] * G[k][c] ----------------------
-// Block tile 64 (r) x 64 (c), k-slab 16, 256 threads with a 4x4 register tile.
-// Shared memory holds the input slab transposed (k-major) so both operands are
-// read as contiguous 4-vectors.
+// Block tile 64 (r) x 64 (c), k-slab 16, 256 threads with a 4x4 register tile
+// (thread (tr, tc) owns 4 rows and the columns 4 tc + j).  Shared memory holds
+// the input slab transposed (k-major).  FP32: the thread's rows are 4 tr + i,
+// read as one 16-byte vector per k (row stride TR + 4 keeps it aligned; a
+// quarter-warp reads 128 contiguous bytes).  FP64: the rows are tr + 16 i,
+// read as 4 scalars per k: the 16 tr of a warp read 16 consecutive doubles, one
+// conflict-free wavefront, where 16-byte vectors of doubles 32 bytes apart
+// would conflict two ways; row stride TR + 1 spreads the slab's stores over
+// the banks.  The two tc of a warp read two broadcast 4-vectors of the factor.
 constexpr int TR = 64, TC = 64, TK = 16;
+
+template <typename T>
+struct AxisRows {
+  static constexpr bool kInterleaved = sizeof(T) == 8;
+  static constexpr int kStride = kInterleaved ? TR + 1 : TR + 4;
+  __device__ static int row(int tr, int i) { return kInterleaved ? tr + 16 * i : 4 * tr + i; }
+};
 
 template <typename T>
 __global__ void __launch_bounds__(256) axis_pass_kernel(const T* __restrict__ in,
                                                         T* __restrict__ out,
                                                         const T* __restrict__ G, int R, int C,
                                                         size_t img_stride) {
-  __shared__ __align__(16) T sA[TK][TR + 4];
+  using Rw = AxisRows<T>;
+  __shared__ __align__(16) T sA[TK][Rw::kStride];
   __shared__ __align__(16) T sB[TK][TC + 4];
   const int tid = threadIdx.x;
   const int tr = tid & 15, tc = tid >> 4;
@@ -56,7 +70,7 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(const T* __restrict__ in
     for (int kk = 0; kk < TK; ++kk) {
       T a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = sA[kk][tr * 4 + i];
+      for (int i = 0; i < 4; ++i) a[i] = sA[kk][Rw::row(tr, i)];
 #pragma unroll
       for (int j = 0; j < 4; ++j) b[j] = sB[kk][tc * 4 + j];
 #pragma unroll
@@ -72,7 +86,7 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(const T* __restrict__ in
     if (c >= C) continue;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      int r = r0 + tr * 4 + i;
+      int r = r0 + Rw::row(tr, i);
       if (r < R) dst[(size_t)c * R + r] = acc[i][j];
     }
   }
