@@ -147,7 +147,13 @@ struct LogOps<float> {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
   }
-  __device__ static float lg(float x) { return log2f(x); }
+  // the hardware base-2 logarithm: absolute error ~2^-22 on log2, below the
+  // FP32 rounding of the result (lg + max) * ln 2 once |result| > 1
+  __device__ static float lg(float x) {
+    float y;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  }
 };
 template <>
 struct LogOps<double> {
@@ -229,11 +235,9 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     T sum = Op::ex(row[c] - m);
     if (SIGNED && !sgn[c]) sum = -sum;
     const T fl = m - Op::kTail;
-    int dmax = 0;
     for (d = 1; d <= dboth; ++d) {
       const T l = lk[d];
       if (l + X < fl) break;
-      dmax = d;
       const T lm = l - m;
       const T ea = Op::ex(lm + row[c - d]), eb = Op::ex(lm + row[c + d]);
       if (SIGNED) sum += (sgn[c - d] ? ea : -ea) + (sgn[c + d] ? eb : -eb);
@@ -243,7 +247,6 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
       for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
         const T l = lk[d];
         if (l + X < fl) break;
-        dmax = d;
         const int k = c + sgnd * d;
         const T ex = Op::ex((l - m) + row[k]);
         sum += (!SIGNED || sgn[k]) ? ex : -ex;
@@ -256,6 +259,7 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     } else {
       out[o] = (Op::lg(sum) + m) * Op::kUnscale;
     }
+    const int dmax = d - 1;  // the last tap distance summed
     n_ex += 1 + min(dmax, c) + min(dmax, C - 1 - c);
   }
   if (exps) {
