@@ -112,7 +112,10 @@ int wdl_log_convolve_signed(wdl_ctx* ctx, const double* log_u, unsigned char* si
  * (:1052-1113).  atoms [K*N] and weights [P*K] are normalised first
  * (Problem::normalize_values, :53-74).
  *   result_la   [P*K]  raw weight gradient of each histogram (resultLa)
- *   result_dic  [K*N]  raw dictionary gradient summed over the P histograms
+ *   result_dic  [K*N]  raw dictionary gradient summed over the P histograms, or
+ *                      NULL when only the weight gradient is wanted (weights
+ *                      fitted onto a fixed dictionary): the kernel-domain forms
+ *                      then skip the dictionary recursion, a third of the work
  *   bary        [P*N]  barycenters, or NULL
  *   loss        [P]    loss of each barycenter against its observation, or NULL
  *   b_init      [P*K*N] initial scalings b[0] (warm restart), or NULL for ones

@@ -420,7 +420,7 @@ int wdl_gradient_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, c
                              double* result_la, double* result_dic, double* bary, double* loss,
                              double* b_last, void* stream) {
   if (!ctx) return WDL_ERR_INVALID_ARG;
-  if (bad_sizes(P, K, L) || !atoms || !weights || !observed || !result_la || !result_dic)
+  if (bad_sizes(P, K, L) || !atoms || !weights || !observed || !result_la)
     return set_error(ctx, WDL_ERR_INVALID_ARG, "bad sizes or NULL required pointer");
   if (loss_type < WDL_LOSS_TV || loss_type > WDL_LOSS_KL)
     return set_error(ctx, WDL_ERR_INVALID_ARG, "loss_type must be 1..4");
@@ -434,7 +434,7 @@ int wdl_gradient_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
                       double* result_la, double* result_dic, double* bary, double* loss,
                       double* b_last) {
   if (!ctx) return WDL_ERR_INVALID_ARG;
-  if (bad_sizes(P, K, L) || !atoms || !weights || !observed || !result_la || !result_dic)
+  if (bad_sizes(P, K, L) || !atoms || !weights || !observed || !result_la)
     return set_error(ctx, WDL_ERR_INVALID_ARG, "bad sizes or NULL required pointer");
   cudaSetDevice(ctx->device);
   const size_t N = ctx->N, KN = (size_t)K * N, PK = (size_t)P * K, PN = (size_t)P * N,
@@ -450,7 +450,7 @@ int wdl_gradient_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
   double* d_obs = c.take<double>(PN);
   double* d_binit = b_init ? c.take<double>(PKN) : nullptr;
   double* d_la = c.take<double>(PK);
-  double* d_dic = c.take<double>(KN);
+  double* d_dic = result_dic ? c.take<double>(KN) : nullptr;
   double* d_bary = bary ? c.take<double>(PN) : nullptr;
   double* d_loss = loss ? c.take<double>(P) : nullptr;
   double* d_blast = b_last ? c.take<double>(PKN) : nullptr;
@@ -463,7 +463,7 @@ int wdl_gradient_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
                                      d_dic, d_bary, d_loss, d_blast, s)))
     return rc;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, d_la, PK * 8, cudaMemcpyDeviceToHost, s));
-  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_dic, d_dic, KN * 8, cudaMemcpyDeviceToHost, s));
+  if (result_dic) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_dic, d_dic, KN * 8, cudaMemcpyDeviceToHost, s));
   if (bary) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(bary, d_bary, PN * 8, cudaMemcpyDeviceToHost, s));
   if (loss) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(loss, d_loss, P * 8, cudaMemcpyDeviceToHost, s));
   if (b_last) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(b_last, d_blast, PKN * 8, cudaMemcpyDeviceToHost, s));

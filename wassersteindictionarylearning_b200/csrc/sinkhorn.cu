@@ -291,14 +291,15 @@ __global__ void k_add_partials(double* __restrict__ dot, const double* __restric
 }
 
 // ---------------- kernel-domain reverse pass (:602-673), one round s ----------------
-// Block per ((p, k), segment): dictionary tmp = (lambda n - v) * b[s]; weights
-// dot += sum_j log(phi[s]) gw (plain log, as :649), u = (lambda gw - r) / phi[s].
+// Block per ((p, k), segment): dictionary tmp = (lambda n - v) * b[s] (when the
+// dictionary recursion runs); weights dot += sum_j log(phi[s]) gw (plain log,
+// as :649), u = (lambda gw - r) / phi[s].
 template <typename T>
 __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
                           const T* __restrict__ b_s, const T* __restrict__ gw,
                           const T* __restrict__ r, const T* __restrict__ phi_s,
                           const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u,
-                          double* __restrict__ part, int K, size_t N) {
+                          double* __restrict__ part, int K, size_t N, int dict) {
   __shared__ double sh[32];
   const size_t pk = blockIdx.x, p = pk / K;
   const T l = lam[pk];
@@ -307,7 +308,7 @@ __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
   double acc = 0;
   for (size_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
     const size_t i = base + j;
-    tmp[i] = (l * n[pb + j] - v[i]) * b_s[i];
+    if (dict) tmp[i] = (l * n[pb + j] - v[i]) * b_s[i];
     const T ph = phi_s[i];
     const T g = gw[pb + j];
     acc += acc_log<T>(ph) * (double)g;
@@ -317,15 +318,19 @@ __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
   if (threadIdx.x == 0) part[pk * gridDim.y + blockIdx.y] = acc;
 }
 
-// gradDic += c / cb[s-1]; tmp = -p c / cb^2; convu *= -p / cb^2 (:612-617, :655-660).
+// gradDic += c / cb[s-1]; tmp = -p c / cb^2 (dictionary recursion, when it
+// runs); convu *= -p / cb^2 (:612-617, :655-660).
 template <typename T>
 __global__ void k_bwd_mid(const T* __restrict__ c, const T* __restrict__ cb,
                           const T* __restrict__ atoms, double* __restrict__ gdic,
-                          T* __restrict__ nxt, size_t KN, size_t PKN, int weights) {
+                          T* __restrict__ nxt, size_t KN, size_t PKN, int weights, int dict) {
   GRID_STRIDE(i, PKN) {
-    const T cbv = cb[i], cc = c[i], pa = atoms[i % KN];
-    gdic[i] += (double)(cc / cbv);
-    nxt[i] = -pa * cc / (cbv * cbv);
+    const T cbv = cb[i], pa = atoms[i % KN];
+    if (dict) {
+      const T cc = c[i];
+      gdic[i] += (double)(cc / cbv);
+      nxt[i] = -pa * cc / (cbv * cbv);
+    }
     if (weights) nxt[PKN + i] = c[PKN + i] * (-pa / (cbv * cbv));
   }
 }
@@ -336,20 +341,22 @@ template <typename T>
 __global__ void k_bwd_post(const T* __restrict__ c2, const T* __restrict__ phi_p,
                            const T* __restrict__ b_p, T* __restrict__ v, T* __restrict__ r,
                            T* __restrict__ n, T* __restrict__ gw, int K, size_t N, size_t PN,
-                           size_t PKN) {
+                           size_t PKN, int dict) {
   GRID_STRIDE(idx, PN) {
     const size_t p = idx / N, j = idx - p * N;
     T sn = T(0), sg = T(0);
     for (int k = 0; k < K; ++k) {
       const size_t i = (p * K + k) * N + j;
-      const T vv = c2[i] / phi_p[i];
-      v[i] = vv;
-      sn += vv;
+      if (dict) {
+        const T vv = c2[i] / phi_p[i];
+        v[i] = vv;
+        sn += vv;
+      }
       const T rr = c2[PKN + i] * b_p[i];
       r[i] = rr;
       sg += rr;
     }
-    n[idx] = sn;
+    if (dict) n[idx] = sn;
     gw[idx] = sg;
   }
 }
@@ -662,7 +669,11 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
   k_loss<T><<<P, 256, 0, s>>>(B.bary, observed, B.wgrad, B.n, B.gw, B.loss, loss_type, N);
   WDL_LAUNCH_CHECK(ctx);
 
-  // Reverse pass, both recursions per round (:602-673 / :730-812).
+  // Reverse pass, both recursions per round (:602-673 / :730-812).  With no
+  // dictionary gradient requested, the kernel domain runs the weight
+  // recursion alone: the operator takes only the second half of each
+  // [dictionary | weights] image pair.
+  const int dict = (result_dic || log_domain) ? 1 : 0;
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.v, 0, PKN * sizeof(T), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.r, 0, PKN * sizeof(T), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, PKN * sizeof(double), s));
@@ -677,18 +688,28 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
     const size_t nimg = (size_t)(more ? 2 : 1) * P * K;
     if (!log_domain) {
       k_bwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
-          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dpart, K, N);
+          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dpart, K, N, dict);
       WDL_LAUNCH_CHECK(ctx);
       k_add_partials<<<(P * K + 127) / 128, 128, 0, s>>>(B.dot, B.dpart, P * K, (int)n_segments(N));
       WDL_LAUNCH_CHECK(ctx);
-      if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
-      k_bwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, PKN, more);
-      WDL_LAUNCH_CHECK(ctx);
+      if (dict) {
+        if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
+      } else if (more) {
+        if ((rc = conv_stack<T>(ctx, u, B.cbuf2 + PKN, B.ctmp, (size_t)P * K, s))) return rc;
+      }
+      if (dict || more) {
+        k_bwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, PKN, more, dict);
+        WDL_LAUNCH_CHECK(ctx);
+      }
       if (!more) break;
-      if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
+      if (dict) {
+        if ((rc = conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, s))) return rc;
+      } else {
+        if ((rc = conv_stack<T>(ctx, u, B.cbuf2 + PKN, B.ctmp, (size_t)P * K, s))) return rc;
+      }
       const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
       const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
-      k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN);
+      k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN, dict);
       WDL_LAUNCH_CHECK(ctx);
     } else {
       k_lbwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
@@ -715,8 +736,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
 
   // Outputs.
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
-  k_sum_over_p<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
-  WDL_LAUNCH_CHECK(ctx);
+  if (result_dic) {
+    k_sum_over_p<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
   if (bary_out) {
     k_cast_back<T><<<G_PN, 256, 0, s>>>(B.bary, bary_out, PN);
     WDL_LAUNCH_CHECK(ctx);
@@ -924,10 +947,13 @@ int gradient_both_fused(wdl_ctx* ctx, int P, int K, int L, int loss_type, const 
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.acc, 0, (size_t)L * PN * 4, s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.nb, 0, 2 * PN * 4, s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gwb, 0, 2 * PN * 4, s));
-  if ((rc = launch_single(ctx, B, P, K, L, loss_type, observed, false, true, s))) return rc;
+  if ((rc = launch_single(ctx, B, P, K, L, loss_type, observed, false, result_dic != nullptr, s)))
+    return rc;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
-  k_sum_over_p_f32<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
-  WDL_LAUNCH_CHECK(ctx);
+  if (result_dic) {
+    k_sum_over_p_f32<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
+    WDL_LAUNCH_CHECK(ctx);
+  }
   const float* acc_L = B.acc + (size_t)(L - 1) * PN;
   if (bary_out) {
     k_exp_to_double<<<launch_cfg(ctx, PN), 256, 0, s>>>(acc_L, bary_out, PN);

@@ -309,10 +309,10 @@ class ServingEngine:
             lam /= lam.sum(axis=1, keepdims=True)
             obs = f64(np.stack([r.observed for r in proj_reqs]))
             la = np.empty(P * K)
-            dic = np.empty(K * N)
             loss = np.empty(P)
+            # weights only: no atom gradient, so the dictionary recursion is skipped
             rc = lib().wdl_gradient_both(ctx, P, K, L, self.loss_type, dptr(f64(s.atoms)),
-                                         dptr(f64(lam)), dptr(obs), None, dptr(la), dptr(dic),
+                                         dptr(f64(lam)), dptr(obs), None, dptr(la), None,
                                          None, dptr(loss), None)
             for i, r in enumerate(proj_reqs):
                 if rc != 0:
