@@ -216,18 +216,22 @@ class ServingEngine:
     def _admit(self):
         """Admit pending requests in arrival order while their iterate stores fit
         the budget.  A request whose shape's context is still being created
-        waits without holding up the requests behind it; one that does not fit
-        (bytes or batch size) holds up everything behind it."""
+        waits, with the later requests of its shape, without holding up the
+        other shapes' requests; one that does not fit (bytes or batch size)
+        holds up everything behind it."""
         with self._lock:
             pending, self._pending = self._pending, deque()
         keep = deque()
         blocked = False
+        waiting = set()  # shapes whose context is not ready: their later requests wait too
         for req in pending:
             if blocked:
                 keep.append(req)
                 continue
-            s = self._ready_shape(self._key(req.shape, self._form(req)))
+            key = self._key(req.shape, self._form(req))
+            s = None if key in waiting else self._ready_shape(key)
             if s is None:
+                waiting.add(key)
                 keep.append(req)
                 continue
             if not req.bytes:
