@@ -38,6 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd Sinkhorn iters/s (128², K=5) vs plain FP32; p50/p99 serve latency"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
+# fused split-BF16 kernel on batched128 (P=64, L=100), from one ncu capture.
+FUSED_DRAM_BYTES_P64_L100 = 28.75e9
 UNIT = "hist-iter/s"
 WORKLOADS = {
     "batched128": dict(name="batched128", P=64, W=128, H=128, K=5, L=100, gamma=1.0, loss=4,
@@ -78,6 +81,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-arms", action="store_true")
     ap.add_argument("--serve-rates", default="50,200,500,2000")
     ap.add_argument("--serve-requests", type=int, default=120)
     # Reduced sizes for profiler captures (the bench line itself uses the workload's).
@@ -387,9 +391,9 @@ def run_ours(args):
         peak_src = "of nominal CUDA-core FMA peak at max clock"
         bound = "fp32-cuda-core" if precision == "fp32" else "fp64-cuda-core"
     if wl["domain"] != "log":
-        # DRAM bytes of one fused launch at P=64, L=100 from one ncu capture
-        # (profiles/sinkhorn_tc_kernel_batched128_dram.md), scaled by P*L
-        traffic = (28.75e9 * (P * L) / (64 * 100)
+        # DRAM bytes (read + write) of one fused launch at P=64, L=100, from a
+        # one-pass ncu capture of this workload, scaled by P*L
+        traffic = (FUSED_DRAM_BYTES_P64_L100 * (P * L) / (64 * 100)
                    if wl["name"] == "batched128" and precision == "split_bf16" else None)
         roofline = dict(bound=bound, achieved=achieved_tflops, peak=peak, unit="TFLOP/s",
                         frac=achieved_tflops / peak, traffic=traffic, peak_source=peak_src,
@@ -438,6 +442,24 @@ def run_ours(args):
         d2h = (n + 1) * 8 + (K * N * 8 if world > 1 else 0)
         e2e = dict(value=units / el, unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h)
 
+    # The other precisions on the same inputs, timed the same way (CUDA events on
+    # the same stream, max over ranks): plain FP32 on the CUDA cores is the
+    # metric's "vs plain FP32"; FP64 on the GPU is the reference's arithmetic.
+    arms, report = None, None
+    if wl["name"] == "batched128" and wl["domain"] == "kernel" and not args.no_arms:
+        outs = {precision: run_outputs(L_, ctx, wl, x_d, obs_d, sd, sptr, dev)}
+        arms = {}
+        for prec in ("fp32", "fp64"):
+            if prec == precision:
+                continue
+            k2 = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=prec, device=local)
+            arms[prec] = time_arm(L_, k2.ctx, wl, x_d, obs_d, sd, sptr, dev, args, world, dist)
+            outs[prec] = run_outputs(L_, k2.ctx, wl, x_d, obs_d, sd, sptr, dev)
+            k2.close()
+            torch.cuda.synchronize()
+        if "fp64" in outs and rank == 0:
+            report = precision_report(outs, wl, x, obs, sd)
+
     serving = None
     if rank == 0 and not args.no_serving and wl["name"] == "batched128":
         serving = [run_serving(float(r), args.serve_requests, local)
@@ -467,7 +489,109 @@ def run_ours(args):
                             objective=fval),
                 roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=int(gpu_launches),
                 clocks=clocks, serving=serving)
+    if arms:
+        for prec, a in arms.items():
+            line[f"value_{prec}"] = a["value"]
+            line[f"ms_per_step_{prec}"] = a["ms_per_step"]
+        if "fp32" in arms:
+            # the metric's comparison: this line's precision over plain FP32 on the GPU
+            line["vs_fp32"] = value / arms["fp32"]["value"]
+        if "fp64" in arms:
+            line["vs_fp64"] = value / arms["fp64"]["value"]
+        line["arms"] = {p: dict(a, precision=p, dtype=dtype_name(p)) for p, a in arms.items()}
+    if report:
+        line["precision_report"] = report
     print(json.dumps(line), flush=True)
+
+
+def time_arm(L_, ctx, wl, x_d, obs_d, sd, sptr, dev, args, world, dist):
+    """One precision's evaluate_both on the bench inputs: warm-up, then the same
+    number of steps as the headline between CUDA events on the same stream."""
+    import torch
+    from wassersteindictionarylearning_b200 import _lib
+    P, K, L = wl["P"], wl["K"], wl["L"]
+    n = x_d.numel()
+    g_d = torch.empty(n, dtype=torch.float64, device=dev)
+    f_d = torch.empty(1, dtype=torch.float64, device=dev)
+
+    def step():
+        _lib.check(L_.wdl_evaluate_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(x_d.data_ptr()),
+                                               C.c_void_p(g_d.data_ptr()), n, C.c_void_p(obs_d.data_ptr()),
+                                               C.c_void_p(f_d.data_ptr()), None, None, None, sptr), ctx)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = P * L * args.steps * world
+    return dict(value=units / (ms / 1e3), ms_per_step=ms / args.steps)
+
+
+def run_outputs(L_, ctx, wl, x_d, obs_d, sd, sptr, dev):
+    """Objective, gradient and barycenters of one evaluation (host copies)."""
+    import torch
+    from wassersteindictionarylearning_b200 import _lib
+    P, K, L, N = wl["P"], wl["K"], wl["L"], wl["W"] * wl["H"]
+    n = x_d.numel()
+    g_d = torch.empty(n, dtype=torch.float64, device=dev)
+    f_d = torch.empty(1, dtype=torch.float64, device=dev)
+    b_d = torch.empty(P * N, dtype=torch.float64, device=dev)
+    _lib.check(L_.wdl_evaluate_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(x_d.data_ptr()),
+                                           C.c_void_p(g_d.data_ptr()), n, C.c_void_p(obs_d.data_ptr()),
+                                           C.c_void_p(f_d.data_ptr()), None, None,
+                                           C.c_void_p(b_d.data_ptr()), sptr), ctx)
+    torch.cuda.synchronize()
+    return dict(f=float(f_d.item()), g=g_d.cpu().numpy(), bary=b_d.cpu().numpy())
+
+
+def precision_report(outs, wl, x, obs, sd, n_scale=4):
+    """Each output's error against the FP64 arm (the GPU FP64 path, which the
+    parity tests hold to the reference within 1e-10): barycenters and the atom
+    gradient normwise (max|a-b| / max|b|), the objective relatively, the weight
+    gradient both normwise and against its floating-point condition scale (the
+    mass of the terms summed into it, from the oracle; computed for the first
+    n_scale histograms, whose weight gradients do not depend on the others)."""
+    import numpy as np
+    P, K, L, W, H = wl["P"], wl["K"], wl["L"], wl["W"], wl["H"]
+    N = W * H
+    PK = P * K
+    ref = outs["fp64"]
+
+    def nrm(a, b):
+        return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+    scale = None
+    try:
+        from oracle.oracle import OracleLib
+        xs = np.concatenate([x[:n_scale * K], x[PK:]])
+        scale = OracleLib().weight_gradient_scale(W, H, 1, wl["gamma"], n_scale, K, L, wl["loss"], sd, xs,
+                                                  obs.reshape(P, N)[:n_scale].reshape(-1))
+    except Exception:  # the oracle's C build is absent: report the normwise errors only
+        scale = None
+    rep = {}
+    for prec, o in outs.items():
+        if prec == "fp64":
+            continue
+        e = dict(barycenter=nrm(o["bary"], ref["bary"]),
+                 objective=abs(o["f"] - ref["f"]) / abs(ref["f"]),
+                 atom_gradient=nrm(o["g"][PK:], ref["g"][PK:]),
+                 weight_gradient_normwise=nrm(o["g"][:PK], ref["g"][:PK]))
+        if scale is not None:
+            d = np.abs(o["g"][:n_scale * K] - ref["g"][:n_scale * K])
+            e["weight_gradient_vs_condition_scale"] = float(np.max(d) / max(float(np.max(scale)), 1e-300))
+        rep[prec] = e
+    rep["against"] = "fp64 arm (GPU FP64, same inputs)"
+    return rep
 
 
 def run_serving(rate, n, device):

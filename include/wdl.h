@@ -225,15 +225,20 @@ int wdl_convolve_device(wdl_ctx* ctx, const double* u, double* out, int nvectors
 /* No counterpart in the reference (which has no device code).  The operator of
  * wdl_convolve_device for callers that cannot allocate device memory while they
  * run (hosts that reserve all memory at start-up, processes under a device
- * memory cap or pool, code building a CUDA graph): it calls no cudaMalloc,
- * cudaFree or other allocating routine, and takes its scratch from one fixed
- * 32 MiB device array inside the library, which every GPU that loads the
- * library holds until the process exits.  The caller passes device input and
+ * memory cap or pool): it calls no cudaMalloc, cudaFree or other allocating
+ * routine, and takes its scratch from one fixed 32 MiB device array inside the
+ * library.  wdl_create reserves that array on the context's device (it looks
+ * up the array's address, which loads the library's module there); the device
+ * holds it until the process exits.  The caller passes device input and
  * output.  3 * nvectors * N * (4 bytes, or 8 for WDL_FP64) rounded up must fit
  * in the 32 MiB, otherwise WDL_ERR_INVALID_ARG (the message gives the limit).
  * All calls share the array: calls that overlap on the GPU race, so serialise
- * them.  The first call on each device looks up the array's device address;
- * make that first call before any stream capture. */
+ * them.  On a tensor-core context with sides above 128 the first call for a
+ * given image count may time the axis pass's tile variants, which synchronises
+ * the stream; wdl_set_autotune(ctx, 0) beforehand keeps the default variant.
+ * CUDA loads each kernel's code on its first launch in the process (lazy
+ * loading); a caller that must see no driver allocation at all runs with
+ * CUDA_MODULE_LOADING=EAGER or makes one call before its no-allocation phase. */
 int wdl_convolve_device_noalloc(wdl_ctx* ctx, const double* u, double* out, int nvectors,
                                 void* stream);
 

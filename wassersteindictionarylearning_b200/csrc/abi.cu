@@ -234,6 +234,7 @@ int wdl_create(wdl_ctx** out, int device, int W, int H, int D, double gamma, int
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_b);
   if (e != cudaSuccess) rc = cuda_error(ctx, e, "stream/event creation");
   if (rc == WDL_OK) rc = build_factors(ctx);
+  if (rc == WDL_OK) rc = noalloc_attach(ctx);
   if (rc == WDL_OK && (precision == WDL_TF32 || precision == WDL_SPLIT_BF16)) {
     rc = tc_init(ctx);
   }

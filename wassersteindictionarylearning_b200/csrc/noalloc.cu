@@ -1,9 +1,8 @@
 // wdl_convolve_device_noalloc: the separable operator for callers that must not
 // allocate device memory while they run — real-time or embedded hosts that
-// reserve all memory up front, processes running under a device-memory cap or
-// a strict pool, and code in the middle of building a CUDA graph, where a
-// cudaMalloc would fail, stall on a device-wide synchronisation, or break the
-// caller's memory budget.
+// reserve all memory up front, and processes running under a device-memory cap
+// or a strict pool, where a cudaMalloc would fail, stall on a device-wide
+// synchronisation, or break the caller's memory budget.
 //
 // The regular entry point (wdl_convolve_device) takes its scratch from the
 // context's grow-only arena, which calls cudaMalloc the first time a size is
@@ -11,43 +10,24 @@
 // calls no allocating routine.  The caller still passes device pointers for
 // the input and output.
 //
-// The array lives in the library's module: every GPU on which the library is
-// loaded holds these kNoAllocScratchBytes until the process exits.  All calls
-// share it, so calls that overlap on the GPU (different streams, or different
-// host threads) race on it; serialise them.  Each call writes every scratch
-// element it reads before reading it, so the array's previous contents never
-// matter and nothing needs clearing.
-#include <mutex>
-
+// The array lives in the library's module, and CUDA loads a module on a
+// device the first time something in it is used.  wdl_create therefore looks
+// up the array's device address (noalloc_attach), which loads the module and
+// reserves the kNoAllocScratchBytes on that device when the context is
+// created, never inside a call of the entry point; the device keeps them until
+// the process exits.  The address is kept per context, so a context created
+// after the device's primary context was reset sees the array where the
+// reloaded module put it.  All calls share the array, so calls that overlap on
+// the GPU (different streams, or different host threads) race on it; serialise
+// them.  Each call writes every scratch element it reads before reading it, so
+// the array's previous contents never matter and nothing needs clearing.
 #include "wdl_internal.cuh"
 
 namespace wdl {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
-constexpr int kMaxDevices = 64;
-
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-
-std::mutex g_scratch_mu;
-void* g_scratch_dev[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device.  In host code
-// g_noalloc_scratch is only a host-side stand-in for the symbol: its address
-// must be looked up per device.  Done once per device, on the first call.
-int scratch_address(wdl_ctx* ctx, void** out) {
-  if (ctx->device < 0 || ctx->device >= kMaxDevices)
-    return set_error(ctx, WDL_ERR_UNSUPPORTED, "device index beyond the no-alloc table");
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev[ctx->device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_scratch_dev[ctx->device] = p;
-  }
-  *out = g_scratch_dev[ctx->device];
-  return WDL_OK;
-}
 
 template <typename T>
 __global__ void k_noalloc_in(const double* __restrict__ in, T* __restrict__ out, size_t n) {
@@ -74,9 +54,9 @@ int convolve_noalloc_t(wdl_ctx* ctx, const double* u, double* out, int nv, cudaS
                          std::to_string(kNoAllocScratchBytes) + " bytes (at most " +
                          std::to_string(max_images) + " images of this grid)");
   }
-  void* base = nullptr;
+  void* base = ctx->noalloc_scratch;
+  if (!base) return set_error(ctx, WDL_ERR_CUDA, "no-allocation scratch array not attached");
   int rc;
-  if ((rc = scratch_address(ctx, &base))) return rc;
   T* a = reinterpret_cast<T*>(base);
   T* b = reinterpret_cast<T*>(static_cast<char*>(base) + part);
   T* t = reinterpret_cast<T*>(static_cast<char*>(base) + 2 * part);
@@ -90,6 +70,18 @@ int convolve_noalloc_t(wdl_ctx* ctx, const double* u, double* out, int nv, cudaS
 }
 
 }  // namespace
+
+// In host code g_noalloc_scratch is only a host-side stand-in for the device
+// symbol; its device address is looked up here, once per context, with the
+// context's device current.
+int noalloc_attach(wdl_ctx* ctx) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+  ctx->noalloc_scratch = p;
+  return WDL_OK;
+}
+
 }  // namespace wdl
 
 extern "C" int wdl_convolve_device_noalloc(wdl_ctx* ctx, const double* u, double* out,

@@ -76,6 +76,9 @@ struct wdl_ctx {
   wdl::Arena io;     // staging of the host-pointer calls
   wdl::TcResources* tc = nullptr;
   int* fused_sync = nullptr;  // status block of the last fused-kernel launch (in the arena)
+  // Device address of the library's fixed no-allocation scratch array on this
+  // context's device, looked up when the context is created (noalloc.cu).
+  void* noalloc_scratch = nullptr;
 
   std::string last_error;
   long long launches = 0;
@@ -118,6 +121,9 @@ int set_error(wdl_ctx* ctx, int code, const std::string& msg);
 bool autotune_enabled();
 int cuda_error(wdl_ctx* ctx, cudaError_t e, const char* where);
 int ensure_arena(wdl_ctx* ctx, size_t bytes);
+// Looks up the no-allocation scratch array's address on the current device
+// into ctx->noalloc_scratch (noalloc.cu); called by wdl_create.
+int noalloc_attach(wdl_ctx* ctx);
 
 #define WDL_CUDA_TRY(ctx, expr)                                    \
   do {                                                             \
