@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-arms", action="store_true")
+    ap.add_argument("--no-regress", action="store_true")
+    ap.add_argument("--regress-iters", type=int, default=3)
     ap.add_argument("--serve-rates", default="50,200,500,2000")
     ap.add_argument("--serve-requests", type=int, default=120)
     # Reduced sizes for profiler captures (the bench line itself uses the workload's).
@@ -460,6 +462,13 @@ def run_ours(args):
         if "fp64" in outs and rank == 0:
             report = precision_report(outs, wl, x, obs, sd)
 
+    # Dictionary learning with the L-BFGS on the device (wdl_regress_both_device):
+    # a few iterations of regress_both on the bench inputs, wall clock on the
+    # device (CUDA events), to report L-BFGS iterations/s beside the evaluations.
+    regress = None
+    if wl["domain"] == "kernel" and not args.no_regress and world == 1:
+        regress = time_regress(L_, ctx, wl, wts, atoms, obs_d, sd, sptr, dev, iters=args.regress_iters)
+
     serving = None
     if rank == 0 and not args.no_serving and wl["name"] == "batched128":
         serving = [run_serving(float(r), args.serve_requests, local)
@@ -488,7 +497,7 @@ def run_ours(args):
                             autotuned=tuned or None,
                             objective=fval),
                 roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=int(gpu_launches),
-                clocks=clocks, serving=serving)
+                clocks=clocks, serving=serving, regress_both_device=regress)
     if arms:
         for prec, a in arms.items():
             line[f"value_{prec}"] = a["value"]
@@ -502,6 +511,32 @@ def run_ours(args):
     if report:
         line["precision_report"] = report
     print(json.dumps(line), flush=True)
+
+
+def time_regress(L_, ctx, wl, wts, atoms, obs_d, sd, sptr, dev, iters=3):
+    """regress_both's optimisation on the device for `iters` L-BFGS iterations
+    (epsilon 1e-50 as the reference sets it, so every iteration runs)."""
+    import numpy as np
+    import torch
+    from wassersteindictionarylearning_b200 import _lib
+    P, K, L = wl["P"], wl["K"], wl["L"]
+    sol = torch.from_numpy(np.concatenate([wts.reshape(-1), atoms.reshape(-1)])).to(dev)
+    status, fval, evals = C.c_int(), C.c_double(), C.c_int()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    _lib.check(L_.wdl_regress_both_device(ctx, P, K, L, wl["loss"], sd, C.c_void_p(sol.data_ptr()),
+                                          C.c_void_p(obs_d.data_ptr()), iters, 1e-50, 0, C.byref(status),
+                                          C.byref(fval), C.byref(evals), sptr), ctx)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    return dict(iterations=iters, evaluations=evals.value, status=status.value, objective=fval.value,
+                ms=ms, lbfgs_iterations_per_s=iters / (ms / 1e3),
+                evaluations_per_s=evals.value / (ms / 1e3),
+                hist_iter_per_s=evals.value * P * L / (ms / 1e3),
+                note="wdl_regress_both_device: every evaluation and L-BFGS step on the device, "
+                     "one 4-byte status read per evaluation")
 
 
 def time_arm(L_, ctx, wl, x_d, obs_d, sd, sptr, dev, args, world, dist):

@@ -132,6 +132,24 @@ int wdl_evaluate_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double s
                       const double* x, double* g, int n, const double* observed, double* f,
                       const double* b_storage, double* b_last, double* bary);
 
+/* WassersteinRegression::regress_both (cpp/inverseWasserstein.h:362-423) with
+ * liblbfgs' algorithm on the device (cpp/lbfgs/lbfgs.c:256-654, strong-Wolfe
+ * backtracking :772-867, m = 6, ftol 1e-4, wolfe 0.9, 20 trials per line
+ * search, the reference's epsilon argument 1e-50 makes it run max_iterations):
+ * solution [n = P*K + K*N] holds the weights and atoms in the original domain
+ * on entry and the optimised, normalised ones on exit (the reference's
+ * transform to [scaled log-weights, log-atoms] and back, :389-401, :424-448).
+ * Every objective evaluation is this context's evaluate_both; the optimisation
+ * vectors (x, gradient, previous point, direction, the 6 correction pairs) stay
+ * on the device and the host reads one status word per evaluation.
+ * warm_restart != 0: runs of 10 iterations, b[L] of each run kept on the device
+ * as the next run's b[0] (:368-384, :407-416; max_iterations >= 10).
+ * status = liblbfgs' return code of the last run, *f its final objective,
+ * *evaluations the objective evaluations (any of the three may be NULL). */
+int wdl_regress_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic, double* solution,
+                     const double* observed, int max_iterations, double epsilon, int warm_restart,
+                     int* status, double* f, int* evaluations);
+
 /* WassersteinBarycenter::compute_barycenter / _log (cpp/inverseWasserstein.h:115-201):
  * forward Bregman projections only, for P weight vectors against one set of atoms.
  * bary [P*N]. */
@@ -221,6 +239,10 @@ int wdl_gradient_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, c
                              double* result_la, double* result_dic, double* bary, double* loss,
                              double* b_last, void* stream);
 int wdl_convolve_device(wdl_ctx* ctx, const double* u, double* out, int nvectors, void* stream);
+/* wdl_regress_both with solution and observed in device memory. */
+int wdl_regress_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                            double* solution, const double* observed, int max_iterations, double epsilon,
+                            int warm_restart, int* status, double* f, int* evaluations, void* stream);
 
 /* No counterpart in the reference (which has no device code).  The operator of
  * wdl_convolve_device for callers that cannot allocate device memory while they
@@ -272,6 +294,20 @@ int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launch
 int wdl_set_autotune(wdl_ctx* ctx, int on);
 int wdl_autotune_count(const wdl_ctx* ctx);
 int wdl_autotune_entry(const wdl_ctx* ctx, int i, long long* key6, int* choice, float* ms);
+/* Failure detection of the fused tensor-core kernel (no reference counterpart;
+ * the reference's only failure signal is a NaN loss that cancels L-BFGS,
+ * cpp/inverseWasserstein.h:1180-1184).  Every wait of that kernel on another
+ * work item is bounded; when a bound runs out the kernel's remaining items stop,
+ * the kernel exits normally and the call returns WDL_ERR_TIMEOUT, with the
+ * context still usable.  wdl_set_wait_limit sets the bound on one dependency
+ * wait, in seconds (0 restores the default of 4 s; at most 60).
+ * wdl_inject_fault(ctx, WDL_FAULT_DROP_FIRST_ITERATION) makes the host leave
+ * the first forward iteration's items out of the next wdl_batch_run's work
+ * table, so that the others wait on flags nothing publishes (one call only;
+ * kind 0 cancels): a fault made on the host for testing that path. */
+enum { WDL_FAULT_DROP_FIRST_ITERATION = 1 };
+int wdl_set_wait_limit(wdl_ctx* ctx, double seconds);
+int wdl_inject_fault(wdl_ctx* ctx, int kind);
 /* Exponentials the log-domain operator evaluated while profiling (the
  * reference evaluates one per tap, N*(W+H) per image; taps whose terms are
  * below the sum's rounding are skipped here). */

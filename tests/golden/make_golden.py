@@ -5,7 +5,15 @@ the reference sources) on small seeded inputs and stores inputs and outputs as
 compressed .npz files.  The reference ships no tests or fixtures of its own, so
 these runs are what pins the oracle and the CUDA path.
 
-    python tests/golden/make_golden.py      # needs oracle/_ref (reference sources present)
+    python tests/golden/make_golden.py           # needs oracle/_ref (reference sources present)
+    python tests/golden/make_golden.py --large   # only the full-grid fixtures (minutes of CPU)
+
+The full-grid fixtures (256x256 log domain, 48^3 kernel domain) do not store
+their inputs: the tests regenerate them from the recorded seeds with
+wassersteindictionarylearning_b200.synthetic and check a few input statistics
+(``in_stats``) first.  Their large outputs are stored as every STRIDE-th entry
+plus the entry count, maximum magnitude, sum and sum of magnitudes of the whole
+array (``sample_stats``), which keeps each fixture well under a megabyte.
 """
 from __future__ import annotations
 
@@ -18,7 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import RefLib  # noqa: E402
+from oracle.oracle import OracleLib, RefLib  # noqa: E402
 from wassersteindictionarylearning_b200.synthetic import (blob_histograms, init_atoms,  # noqa: E402
                                                           init_weights, scale_dictionary,
                                                           to_variables)
@@ -30,7 +38,89 @@ def save(name, **arrays):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+STRIDE = 16
+
+
+def sample_stats(a, stride=STRIDE):
+    a = np.asarray(a, dtype=np.float64).reshape(-1)
+    return dict(sample=a[::stride].copy(), n=a.size, absmax=float(np.max(np.abs(a))),
+                total=float(np.sum(a)), abssum=float(np.sum(np.abs(a))), stride=stride)
+
+
+def in_stats(*arrays):
+    return np.array([v for a in arrays for v in (float(np.sum(a)), float(np.sum(np.asarray(a) ** 2)),
+                                                  float(np.max(a)), float(np.min(a)))])
+
+
+def save_stats(name, prefix, a, out):
+    for k, v in sample_stats(a).items():
+        out[f"{prefix}_{k}"] = v
+
+
+def large():
+    """Full-grid fixtures: the log-domain configuration's grid (256x256, K=8,
+    gamma 0.5, TV loss, 1-3 sharp blobs of std 0.01-0.04 of the side) at the
+    reduced P and L of a CPU run, its signed operator alone, and the serving
+    volume (48^3, K=5, L=50, gamma 2) in the kernel domain."""
+    R = RefLib()
+    O = OracleLib()  # condition scales of the weight gradients (the reference has no such output)
+    # compute_gradient_both_log_signArray (cpp/inverseWasserstein.h:678-814), one histogram
+    W = H = 256
+    N = W * H
+    K, L, g, lt = 8, 10, 0.5, 1
+    obs = blob_histograms(1, W, H, n_blobs=(1, 3), std_frac=(0.01, 0.04), seed=71)[0]
+    atoms = init_atoms(K, N, seed=72)
+    lam = init_weights(1, K, seed=73)[0]
+    la, dic, bary = R.gradient_both_log(W, H, g, K, L, lt, atoms, lam, obs)
+    out = dict(W=W, H=H, K=K, L=L, gamma=g, loss=lt, seeds=np.array([71, 72, 73]),
+               in_stats=in_stats(obs, atoms, lam), lambdas=lam, resultLa=la, bary=bary)
+    save_stats("gradlog_256x256_K8_L10_loss1", "resultDic", dic, out)
+    save("full_gradlog_256x256_K8_L10_loss1", **out)
+
+    # evaluate_both in the log domain over P = 2 histograms (:986-1145)
+    P = 2
+    obs = blob_histograms(P, W, H, n_blobs=(1, 3), std_frac=(0.01, 0.04), seed=81)
+    atoms = init_atoms(K, N, seed=82)
+    w = init_weights(P, K, seed=83)
+    sd = scale_dictionary(N, P)
+    x = to_variables(w, atoms, sd)
+    f, gr = R.evaluate_both(W, H, 1, g, P, K, L, lt, sd, x, obs, log_domain=True)
+    out = dict(P=P, W=W, H=H, K=K, L=L, gamma=g, loss=lt, scale_dic=sd, seeds=np.array([81, 82, 83]),
+               in_stats=in_stats(obs, atoms, w), f=f, g_weights=gr[:P * K],
+               g_weights_scale=O.weight_gradient_scale(W, H, 1, g, P, K, L, lt, sd, x, obs, log_domain=True))
+    save_stats("eval_P2_256x256_K8_L10_loss1_log", "g_atoms", gr[P * K:], out)
+    save("full_eval_P2_256x256_K8_L10_loss1_log", **out)
+
+    # log_convolve and log_convolve_signArray alone (cpp/kernels.h:1073-1163)
+    rng = np.random.Generator(np.random.PCG64(91))
+    u = np.log(rng.random(N)) * 3.0
+    sg = rng.integers(0, 256, (N + 7) // 8).astype(np.uint8)
+    out_s, signs_out = R.log_convolve_signed(W, H, g, u, sg, 1)
+    out = dict(W=W, H=H, gamma=g, nv=1, seed=91, in_stats=in_stats(u), signs_in=sg, signs_out=signs_out)
+    save_stats("logconv_256x256_g0.5", "out", R.log_convolve(W, H, g, u, 1), out)
+    save_stats("logconv_256x256_g0.5", "out_signed", out_s, out)
+    save("full_logconv_256x256_g0.5", **out)
+
+    # the serving volume in the kernel domain: compute_gradient_both on 48^3 (Gaussian3DKernel)
+    W = H = D = 48
+    N = W * H * D
+    K, L, g, lt = 5, 50, 2.0, 2
+    obs = blob_histograms(1, W, H, D, n_blobs=(1, 3), std_frac=(0.05, 0.12), seed=101)[0]
+    atoms = init_atoms(K, N, seed=102)
+    lam = init_weights(1, K, seed=103)[0]
+    la, dic, bary = R.gradient_both(W, H, D, g, K, L, lt, atoms, lam, obs)
+    out = dict(W=W, H=H, D=D, K=K, L=L, gamma=g, loss=lt, seeds=np.array([101, 102, 103]),
+               in_stats=in_stats(obs, atoms, lam), lambdas=lam, resultLa=la,
+               resultLa_scale=O.gradient_both_scale(W, H, D, g, K, L, lt, atoms, lam, obs))
+    save_stats("grad_48x48x48_K5_L50_loss2", "bary", bary, out)
+    save_stats("grad_48x48x48_K5_L50_loss2", "resultDic", dic, out)
+    save("full_grad_48x48x48_K5_L50_loss2", **out)
+
+
 def main():
+    if "--large" in sys.argv:
+        large()
+        return
     R = RefLib()
     rng = np.random.Generator(np.random.PCG64(1234))
 

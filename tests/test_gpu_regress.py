@@ -1,0 +1,72 @@
+"""GPU: regress_both with the L-BFGS on the device (wdl_regress_both).
+
+The device optimisation must land where the reference's regress_both does
+(golden regress_*, FP64, four iterations, 1e-8), follow the host L-BFGS
+restatement driving the same context's evaluate_both (the same algorithm with
+the vectors on the host), and carry the warm-restart scalings between runs as
+the reference does (cpp/inverseWasserstein.h:362-423)."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _regression(W, H, gamma, P, K, L, loss, sd, obs, precision):
+    from wassersteindictionarylearning_b200 import CudaGaussian2DKernel, Problem, WassersteinRegression
+    k = CudaGaussian2DKernel(gamma, W, H, precision=precision)
+    return WassersteinRegression(Problem(np.ones((K, W * H)), obs, k, None, P), L, loss, sd)
+
+
+def test_device_regress_matches_reference_golden():
+    (_, f), = golden("regress_*")
+    W, H, P, K, L = (int(f[k]) for k in ("W", "H", "P", "K", "L"))
+    reg = _regression(W, H, float(f["gamma"]), P, K, L, int(f["loss"]), float(f["scale_dic"]), f["obs"],
+                      "fp64")
+    reg.wrTotalIteration = int(f["iters"])
+    sol = f["solution0"].copy()
+    status = reg.regress_both_device(sol)
+    assert status == -997  # LBFGSERR_MAXIMUMITERATION: epsilon 1e-50 runs every iteration
+    assert rel(sol, f["solution"]) < 1e-8
+    assert reg.device_evaluations >= int(f["iters"]) + 1
+
+
+def _case(P=4, W=32, H=24, K=3, L=12, gamma=2.0, loss=2, seed=3):
+    from wassersteindictionarylearning_b200.synthetic import make_problem
+    cfg, obs, atoms, w = make_problem(None, seed=seed, P=P, W=W, H=H, K=K, L=L, gamma=gamma, loss=loss)
+    sol0 = np.concatenate([w.reshape(-1), atoms.reshape(-1)])
+    return cfg, obs, sol0
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 1e-5), ("split_bf16", 1e-3)])
+def test_device_regress_follows_host_lbfgs(precision, tol):
+    cfg, obs, sol0 = _case()
+    args = (cfg["W"], cfg["H"], cfg["gamma"], cfg["P"], cfg["K"], cfg["L"], 2, cfg["scale_dic"], obs, precision)
+    host = _regression(*args)
+    host.wrTotalIteration = 6
+    s_host = sol0.copy()
+    st_host = host.regress_both(s_host)
+    dev = _regression(*args)
+    dev.wrTotalIteration = 6
+    s_dev = sol0.copy()
+    st_dev = dev.regress_both_device(s_dev)
+    assert st_dev == st_host
+    assert rel(s_dev, s_host) < tol
+    assert np.allclose(s_dev[: cfg["P"] * cfg["K"]].reshape(cfg["P"], -1).sum(axis=1), 1.0)
+
+
+def test_device_regress_warm_restart_matches_host():
+    cfg, obs, sol0 = _case(P=2, W=16, H=16, K=2, L=6, seed=5)
+    args = (cfg["W"], cfg["H"], cfg["gamma"], cfg["P"], cfg["K"], cfg["L"], 2, cfg["scale_dic"], obs, "fp64")
+    host = _regression(*args)
+    host.warmRestart = True
+    host.wrTotalIteration = 20
+    s_host = sol0.copy()
+    host.regress_both(s_host)
+    dev = _regression(*args)
+    dev.warmRestart = True
+    dev.wrTotalIteration = 20
+    s_dev = sol0.copy()
+    dev.regress_both_device(s_dev)
+    assert rel(s_dev, s_host) < 1e-8

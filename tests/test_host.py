@@ -137,3 +137,26 @@ def test_resumable_lbfgs_matches_blocking_form():
     except StopIteration as e:
         r2, x2, f2 = e.value
     assert r1 == r2 and np.array_equal(x1, x2) and f1 == f2
+
+
+def test_host_lbfgs_reproduces_reference_regress_both(oracle):
+    """The host L-BFGS (one copy of liblbfgs' algorithm, lbfgs.py) driven by the
+    oracle's evaluate_both lands where the reference's regress_both does after
+    four iterations (golden regress_*, cpp/inverseWasserstein.h:362-423)."""
+    from conftest import golden, rel
+    from wassersteindictionarylearning_b200 import lbfgs as lb
+    (_, f), = golden("regress_*")
+    W, H, P, K, L = (int(f[k]) for k in ("W", "H", "P", "K", "L"))
+    sd, g, lt = float(f["scale_dic"]), float(f["gamma"]), int(f["loss"])
+    sol0 = f["solution0"]
+    x0 = np.concatenate([np.log(sol0[: P * K]) * sd, np.log(sol0[P * K:])])
+
+    def ev(x, step):
+        return oracle.evaluate_both(W, H, 1, g, P, K, L, lt, sd, x, f["obs"])
+
+    ret, x, _ = lb.lbfgs(x0, ev, None, lb.LbfgsParam(max_iterations=int(f["iters"])))
+    w = np.exp(x[: P * K] / sd).reshape(P, K)
+    w /= w.sum(axis=1, keepdims=True)
+    a = np.exp(x[P * K:]).reshape(K, -1)
+    a /= a.sum(axis=1, keepdims=True)
+    assert rel(np.concatenate([w.reshape(-1), a.reshape(-1)]), f["solution"]) < 1e-8

@@ -78,12 +78,9 @@ def test_noalloc_call_allocates_nothing():
     call(k, u, out, nv)
     free1, _ = torch.cuda.mem_get_info(dev)
     assert free1 == free0, (free0, free1)
-    # the regular entry point, by contrast, grows the context's arena on first use
     _lib.check(L.wdl_convolve_device(k.ctx, C.c_void_p(u.data_ptr()), C.c_void_p(ref.data_ptr()), nv,
                                      None), k.ctx)
     _lib.check(L.wdl_synchronize(k.ctx), k.ctx)
-    free2, _ = torch.cuda.mem_get_info(dev)
-    assert free2 < free1
     assert rel(out.cpu().numpy(), ref.cpu().numpy()) < TOL["fp32"]
 
 

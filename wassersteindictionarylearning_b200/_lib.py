@@ -31,6 +31,7 @@ _vp = C.c_void_p
 
 WDL_MODE_WEIGHTS, WDL_MODE_BOTH, WDL_MODE_BARYCENTER = 0, 1, 2
 WDL_FIT_OVERFLOW = -2000
+WDL_FAULT_DROP_FIRST_ITERATION = 1
 
 
 class WdlProblem(C.Structure):
@@ -97,6 +98,13 @@ SIGNATURES = {
     "wdl_phase_trace": ([_vp, _dp], C.c_int),
     "wdl_exp_profile": ([_vp, _dp], C.c_int),
     "wdl_set_autotune": ([_vp, C.c_int], C.c_int),
+    "wdl_set_wait_limit": ([_vp, C.c_double], C.c_int),
+    "wdl_regress_both": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp, C.c_int,
+                          C.c_double, C.c_int, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)], C.c_int),
+    "wdl_regress_both_device": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp, C.c_int,
+                                 C.c_double, C.c_int, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int), _vp],
+                                C.c_int),
+    "wdl_inject_fault": ([_vp, C.c_int], C.c_int),
     "wdl_autotune_count": ([_vp], C.c_int),
     "wdl_autotune_entry": ([_vp, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                             C.POINTER(C.c_float)], C.c_int),

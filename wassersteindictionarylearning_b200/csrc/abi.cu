@@ -258,6 +258,7 @@ int wdl_destroy(wdl_ctx* ctx) {
     if (ctx->G32[a]) cudaFree(ctx->G32[a]);
   }
   if (ctx->arena.ptr) cudaFree(ctx->arena.ptr);
+  if (ctx->lbfgs_arena.ptr) cudaFree(ctx->lbfgs_arena.ptr);
   if (ctx->d_trace) cudaFree(ctx->d_trace);
   if (ctx->d_taps) cudaFree(ctx->d_taps);
   for (auto& gr : ctx->graphs)
@@ -307,6 +308,22 @@ int wdl_phase_trace(wdl_ctx* ctx, double* out27) {
 int wdl_set_autotune(wdl_ctx* ctx, int on) {
   if (!ctx) return WDL_ERR_INVALID_ARG;
   ctx->autotune = on != 0;
+  return WDL_OK;
+}
+
+int wdl_set_wait_limit(wdl_ctx* ctx, double seconds) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  if (!(seconds >= 0) || seconds > 60)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "wait limit must be in [0, 60] seconds (0: default)");
+  ctx->wait_limit_s = seconds;
+  return WDL_OK;
+}
+
+int wdl_inject_fault(wdl_ctx* ctx, int kind) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  if (kind != 0 && kind != WDL_FAULT_DROP_FIRST_ITERATION)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "unknown fault kind");
+  ctx->inject_fault = kind;
   return WDL_OK;
 }
 
@@ -483,6 +500,55 @@ int wdl_evaluate_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, d
   cudaSetDevice(ctx->device);
   return evaluate_both_dev(ctx, P, K, L, loss_type, scale_dic, x, g, n, observed, f, b_storage,
                            b_last, bary, pick(ctx, stream));
+}
+
+static int regress_args(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                        const double* solution, const double* observed, int max_iterations) {
+  if (bad_sizes(P, K, L) || !solution || !observed || !(scale_dic != 0) || !std::isfinite(scale_dic))
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "bad sizes, scale or NULL required pointer");
+  if (loss_type < WDL_LOSS_TV || loss_type > WDL_LOSS_KL)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "loss_type must be 1..4");
+  if (max_iterations < 0) return set_error(ctx, WDL_ERR_INVALID_ARG, "max_iterations must be >= 0");
+  return WDL_OK;
+}
+
+int wdl_regress_both_device(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,
+                            double* solution, const double* observed, int max_iterations, double epsilon,
+                            int warm_restart, int* status, double* f, int* evaluations, void* stream) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = regress_args(ctx, P, K, L, loss_type, scale_dic, solution, observed, max_iterations))) return rc;
+  if (warm_restart && max_iterations < 10)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "warm restart runs 10-iteration runs: max_iterations >= 10");
+  cudaSetDevice(ctx->device);
+  return regress_both_dev(ctx, P, K, L, loss_type, scale_dic, solution, observed, max_iterations, epsilon,
+                          warm_restart, status, f, evaluations, pick(ctx, stream));
+}
+
+int wdl_regress_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic, double* solution,
+                     const double* observed, int max_iterations, double epsilon, int warm_restart,
+                     int* status, double* f, int* evaluations) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = regress_args(ctx, P, K, L, loss_type, scale_dic, solution, observed, max_iterations))) return rc;
+  if (warm_restart && max_iterations < 10)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "warm restart runs 10-iteration runs: max_iterations >= 10");
+  cudaSetDevice(ctx->device);
+  const size_t N = ctx->N, n = (size_t)P * K + (size_t)K * N, PN = (size_t)P * N;
+  Io& io = io_of(ctx);
+  if ((rc = ensure_io(ctx, io, rnd(n * 8) + rnd(PN * 8) + 256))) return rc;
+  Carver c{static_cast<char*>(io.ptr)};
+  double* d_sol = c.take<double>(n);
+  double* d_obs = c.take<double>(PN);
+  cudaStream_t s = ctx->stream;
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_sol, solution, n * 8, cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_obs, observed, PN * 8, cudaMemcpyHostToDevice, s));
+  if ((rc = regress_both_dev(ctx, P, K, L, loss_type, scale_dic, d_sol, d_obs, max_iterations, epsilon,
+                             warm_restart, status, f, evaluations, s)))
+    return rc;
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(solution, d_sol, n * 8, cudaMemcpyDeviceToHost, s));
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return WDL_OK;
 }
 
 int wdl_evaluate_both(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic,

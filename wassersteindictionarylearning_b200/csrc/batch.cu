@@ -326,6 +326,15 @@ extern "C" int wdl_batch_run(wdl_ctx* ctx, const wdl_problem* pb, int nprob) {
   std::vector<int4> items;
   batch_items(bp, nullptr, items);
   if (items.size() != bp.n_items_all) return set_error(ctx, WDL_ERR_INVALID_ARG, "internal: item count mismatch");
+  if (ctx->inject_fault == WDL_FAULT_DROP_FIRST_ITERATION) {
+    // host-side fault (wdl_inject_fault): no item of the first forward
+    // iteration runs, so every other item waits on a flag nothing publishes
+    std::vector<int4> kept;
+    for (const int4& it : items)
+      if (!(it.y == 0 && it.z == 1)) kept.push_back(it);
+    items.swap(kept);
+    ctx->inject_fault = 0;
+  }
   char* base = bp.base;
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(base + bp.items_off, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
   if ((rc = batch_launch(ctx, bp, items.size(), s))) return rc;

@@ -41,7 +41,7 @@ namespace wdl {
 namespace {
 using namespace tc;
 
-constexpr uint64_t kDepWaitNs = 4000000000ull;  // bound on a dependency wait
+constexpr uint64_t kDepWaitNs = 4000000000ull;  // default bound on a dependency wait
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -51,13 +51,13 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ bool wait_ge(const int* flag, int target) {
+__device__ bool wait_ge(const int* flag, int target, uint64_t limit_ns) {
   if (ld_acquire(flag) >= target) return true;
   const uint64_t t0 = ptx::globaltimer_ns();
   while (true) {
     __nanosleep(100);
     if (ld_acquire(flag) >= target) return true;
-    if (ptx::globaltimer_ns() - t0 > kDepWaitNs) return false;
+    if (ptx::globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -85,10 +85,73 @@ __device__ __forceinline__ double st_sum(double v, double* scratch, int st, int 
 }
 
 // Pulls an image's 128-byte lines into L2 ahead of use (no registers, no wait).
+#ifndef WDL_X_BULKPF
+#define WDL_X_BULKPF 0
+#endif
 __device__ __forceinline__ void prefetch_l2(const float* p, size_t n, int t) {
+#if WDL_X_BULKPF
+  // one bulk prefetch by the copy engine: the 16-byte aligned interior of the image
+  if (t == 0) {
+    const uintptr_t a0 = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t a1 = (reinterpret_cast<uintptr_t>(p + n)) & ~uintptr_t(15);
+    if (a1 > a0)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((uint32_t)(a1 - a0)) : "memory");
+  }
+#else
   for (size_t off = (size_t)t * 32; off < n; off += (size_t)kSt * 32)
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
+#endif
 }
+
+// L2 eviction priority of a global access: normal, evict-first (the last use
+// of a streamed tape image) or evict-last (the reverse pass's working images).
+#ifndef WDL_X_HINTS
+#define WDL_X_HINTS 0
+#endif
+enum : int { kHN = 0, kHF = 1, kHL = 2 };
+template <int HINT>
+__device__ __forceinline__ uint64_t l2pol() {
+  uint64_t p;
+  if (HINT == kHF) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  else asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+template <int HINT>
+__device__ __forceinline__ float4 ldg4(const float* a) {
+  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) return __ldcg(reinterpret_cast<const float4*>(a));
+  float4 v;
+  asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(a), "l"(l2pol<HINT>()));
+  return v;
+}
+template <int HINT>
+__device__ __forceinline__ float ldg1(const float* a) {
+  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) return __ldcg(a);
+  float v;
+  asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(l2pol<HINT>()));
+  return v;
+}
+template <int HINT>
+__device__ __forceinline__ void stg4(float* a, float4 v) {
+  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) { __stcg(reinterpret_cast<float4*>(a), v); return; }
+  asm volatile("st.global.cg.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "f"(v.x), "f"(v.y),
+               "f"(v.z), "f"(v.w), "l"(l2pol<HINT>())
+               : "memory");
+}
+template <int HINT>
+__device__ __forceinline__ void stg1(float* a, float v) {
+  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) { __stcg(a, v); return; }
+  asm volatile("st.global.cg.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(l2pol<HINT>()) : "memory");
+}
+// Hints of up to 4 inputs, 2 bits each.
+constexpr uint32_t hints(int a = kHN, int b = kHN, int c = kHN, int d = kHN) {
+  return (uint32_t)a | ((uint32_t)b << 2) | ((uint32_t)c << 4) | ((uint32_t)d << 6);
+}
+template <uint32_t HS, int A>
+struct HintOf {
+  static constexpr int v = (int)((HS >> (2 * A)) & 3u);
+};
 
 // Phase trace (thread 0 of a stream; only when a trace buffer is given):
 // claim, dependency wait, prologue, first convolution, mid, second
@@ -115,11 +178,32 @@ struct Geo {
   bool vec;
 };
 
+template <int NIN, int CE, uint32_t HS, int A>
+__device__ __forceinline__ void load_row_chunk(float (&in)[NIN > 0 ? NIN : 1][CE],
+                                               const float* const (&src)[NIN > 0 ? NIN : 1], int i, int x0,
+                                               bool row_ok, const Geo& g) {
+  if constexpr (A < NIN) {
+    constexpr int H = HintOf<HS, A>::v;
+    const float* row = src[A] + (size_t)i * g.W;
+    if (row_ok && g.vec && x0 + CE <= g.W) {
+#pragma unroll
+      for (int q = 0; q < CE; q += 4) {
+        const float4 f4 = ldg4<H>(row + x0 + q);
+        in[A][q] = f4.x; in[A][q + 1] = f4.y; in[A][q + 2] = f4.z; in[A][q + 3] = f4.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < CE; ++q) in[A][q] = (row_ok && x0 + q < g.W) ? ldg1<H>(row + x0 + q) : 0.f;
+    }
+    load_row_chunk<NIN, CE, HS, A + 1>(in, src, i, x0, row_ok, g);
+  }
+}
+
 // Stage the column-form operand X1(i, x) = f(in_0..in_{NIN-1} at (i, x)) for
 // rows i < Hp, x < Wp (zero outside the H x W image).  UNR chunks of loads are
 // issued before any is consumed.  f may accumulate side sums (captured by
 // reference); it is only called for pixels inside the image.
-template <bool SPLIT, int NIN, class F>
+template <bool SPLIT, int NIN, uint32_t HS = 0, class F>
 __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
                                            F f, const Geo& g, int t) {
   constexpr int CE = SPLIT ? 8 : 4;
@@ -136,20 +220,7 @@ __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&s
       iu[u] = i;
       xu[u] = x0;
       const bool row_ok = c < total && i < g.H;
-#pragma unroll
-      for (int a = 0; a < NIN; ++a) {
-        const float* row = src[a] + (size_t)i * g.W;
-        if (row_ok && g.vec && x0 + CE <= g.W) {
-#pragma unroll
-          for (int q = 0; q < CE; q += 4) {
-            const float4 f4 = __ldcg(reinterpret_cast<const float4*>(row + x0 + q));
-            in[u][a][q] = f4.x; in[u][a][q + 1] = f4.y; in[u][a][q + 2] = f4.z; in[u][a][q + 3] = f4.w;
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < CE; ++q) in[u][a][q] = (row_ok && x0 + q < g.W) ? __ldcg(row + x0 + q) : 0.f;
-        }
-      }
+      load_row_chunk<NIN, CE, HS, 0>(in[u], src, i, x0, row_ok, g);
     }
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
@@ -220,19 +291,27 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
 // are loaded first (all loads in flight together), then m(idx, y, in) consumes
 // them (it may store) and returns the next operand's value, written as row x
 // (K = i) of the tile when stage_next.
-template <bool SPLIT, int NIN, class M>
+template <int NIN, uint32_t HS, int A>
+__device__ __forceinline__ void load_col_chunk(float (&in)[NIN][16], const float* const (&src)[NIN], int c0,
+                                               int x, const Geo& g) {
+  if constexpr (A < NIN) {
+    constexpr int H = HintOf<HS, A>::v;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int i = c0 + t;
+      in[A][t] = (x < g.W && i < g.H) ? ldg1<H>(src[A] + (size_t)i * g.W + x) : 1.f;
+    }
+    load_col_chunk<NIN, HS, A + 1>(in, src, c0, x, g);
+  }
+}
+
+template <bool SPLIT, int NIN, uint32_t HS = 0, class M>
 __device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
                                             bool stage_next) {
   const int x = c.lane_row;
   for (int c0 = 16 * c.half; c0 < g.Hp; c0 += 32) {
     float in[NIN][16];
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const int i = c0 + t;
-      const bool ok = x < g.W && i < g.H;
-#pragma unroll
-      for (int q = 0; q < NIN; ++q) in[q][t] = ok ? __ldcg(src[q] + (size_t)i * g.W + x) : 1.f;
-    }
+    load_col_chunk<NIN, HS, 0>(in, src, c0, x, g);
     float y[16];
     ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
     ptx::tmem_ld_wait();
@@ -248,10 +327,32 @@ __device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* c
   }
 }
 
+template <int NIN, uint32_t HS, int A>
+__device__ __forceinline__ void load_px4(float (&in)[NIN > 0 ? NIN : 1][4], const float* const (&src)[NIN > 0 ? NIN : 1],
+                                         size_t idx, bool okr, int x0, const Geo& g) {
+  if constexpr (A < NIN) {
+    constexpr int H = HintOf<HS, A>::v;
+    if (okr && g.vec) {
+      const float4 f = ldg4<H>(src[A] + idx);
+      in[A][0] = f.x; in[A][1] = f.y; in[A][2] = f.z; in[A][3] = f.w;
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) in[A][r] = (okr && x0 + r < g.W) ? ldg1<H>(src[A] + idx + r) : 1.f;
+    }
+    load_px4<NIN, HS, A + 1>(in, src, idx, okr, x0, g);
+  }
+}
+
+template <int HINT = kHN>
 __device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
-               "f"(d)
-               : "memory");
+  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+  } else {
+    asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(a), "f"(b),
+                 "f"(c), "f"(d), "l"(l2pol<HINT>())
+                 : "memory");
+  }
 }
 __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x) : (float)kLogEpsilon; }
 
@@ -262,9 +363,12 @@ __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x)
 // cover one row, so every global load, store and red is a contiguous 512-byte
 // row.  e(idx, y4, in4) gets 4 consecutive pixels, may store, and returns the
 // 4 values added into acc[idx..idx+3].
-template <int NIN, class E>
+#ifndef WDL_X_ROT
+#define WDL_X_ROT 0
+#endif
+template <int NIN, uint32_t HS = 0, int RH = kHN, class E>
 __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
-                                             float* acc, E e) {
+                                             float* acc, E e, int rot = 0) {
   {
     const int i = c.lane_row;
     uint8_t* rowp = c.tile + (size_t)i * 512;
@@ -287,33 +391,32 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
   for (int i0 = c.t >> 5; i0 < g.H; i0 += kWarps * U) {
     float4 y4[U];
     float in[U][NIN > 0 ? NIN : 1][4];
+    int iu[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * kWarps;
+      int i = i0 + u * kWarps;
+#if WDL_X_ROT
+      // rows in an order rotated per atom, so that the K items reducing into
+      // the same image at the same time add into different rows
+      if (i < g.H) { i += rot; if (i >= g.H) i -= g.H; }
+      else i = g.H;
+#endif
+      iu[u] = i;
       const bool okr = i < g.H && x0 < g.W;
       y4[u] = okr ? *reinterpret_cast<const float4*>(c.tile + (size_t)i * 512 + ((j ^ (i & 7)) << 4))
                   : make_float4(0.f, 0.f, 0.f, 0.f);
       const size_t idx = (size_t)i * g.W + x0;
-#pragma unroll
-      for (int q = 0; q < NIN; ++q) {
-        if (okr && g.vec) {
-          const float4 f = __ldcg(reinterpret_cast<const float4*>(src[q] + idx));
-          in[u][q][0] = f.x; in[u][q][1] = f.y; in[u][q][2] = f.z; in[u][q][3] = f.w;
-        } else {
-#pragma unroll
-          for (int r = 0; r < 4; ++r) in[u][q][r] = (okr && x0 + r < g.W) ? __ldcg(src[q] + idx + r) : 1.f;
-        }
-      }
+      load_px4<NIN, HS, 0>(in[u], src, idx, okr, x0, g);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * kWarps;
+      const int i = iu[u];
       if (i >= g.H || x0 >= g.W) continue;
       const size_t idx = (size_t)i * g.W + x0;
       const int nv = g.W - x0 < 4 ? g.W - x0 : 4;
       const float4 out = e(idx, y4[u], in[u], nv);
       if (g.vec) {
-        red_add4(acc + idx, out.x, out.y, out.z, out.w);
+        red_add4<RH>(acc + idx, out.x, out.y, out.z, out.w);
       } else {
         const float o[4] = {out.x, out.y, out.z, out.w};
         for (int r = 0; r < nv; ++r) atomicAdd(acc + idx + r, o[r]);
@@ -323,12 +426,13 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
 }
 
 // Stores 4 consecutive values (nv valid; 16-byte store when the row is aligned).
+template <int HINT = kHN>
 __device__ __forceinline__ void st4(float* p, float4 v, int nv, bool vec) {
   if (vec) {
-    __stcg(reinterpret_cast<float4*>(p), v);
+    stg4<HINT>(p, v);
   } else {
     const float o[4] = {v.x, v.y, v.z, v.w};
-    for (int r = 0; r < nv; ++r) __stcg(p + r, o[r]);
+    for (int r = 0; r < nv; ++r) stg1<HINT>(p + r, o[r]);
   }
 }
 
@@ -475,9 +579,9 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     if (t == 0) {
       bool ok = true;
       if (type == 0) {
-        if (step > 1) ok = wait_ge(&bary_ready[p], step - 1);
+        if (step > 1) ok = wait_ge(&bary_ready[p], step - 1, a.dep_wait_ns);
       } else {
-        ok = wait_ge(&msg_ready[p], L - step);
+        ok = wait_ge(&msg_ready[p], L - step, a.dep_wait_ns);
       }
       s_int[st * 4 + 1] = ok ? 1 : 0;
     }
@@ -488,6 +592,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     }
     tr.mark(1);
     const float lam = pr->lam[pk];
+    const int rot = WDL_X_ROT ? (k * g.H) / K : 0;
     const float* atom = pr->atoms + (size_t)k * N;
     bool ok = true;
 
@@ -521,8 +626,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       tr.mark(3);
       const bool keep_cb = !fwd_only;
       const float* msrc[1] = {atom};
-      mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
-        if (keep_cb) __stcg(cb_out + idx, y);
+      mid_columns<SPLIT, 1, hints(kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
+        if (keep_cb) stg1<kHF>(cb_out + idx, y);  // read again only in the reverse pass
         return fdiv(in[0], y);
       }, true);
       tr.mark(4);
@@ -535,26 +640,26 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         for (int r = 0; r < nv; ++r) bad |= !(o[r] > 0.f && o[r] <= FLT_MAX);
         return make_float4(lam * safe_logf(y.x), lam * safe_logf(y.y), lam * safe_logf(y.z),
                            lam * safe_logf(y.w));
-      });
+      }, rot);
       if (bad) *(volatile int*)(range + p) = 1;
       tr.mark(6);
     } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
       const int s = step;
       const float* src[4] = {pr->nb + (size_t)(s & 1) * PN + (size_t)p * N, pr->v + pk * N,
                              pr->acc + slot(s) * PN + (size_t)p * N, pr->phi + slot(s) * PKN + pk * N};
-      stage_rows<SPLIT, 4>(c.tile, src,
-                           [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); },
-                           g, t);
+      stage_rows<SPLIT, 4, hints(kHL, kHL, kHF, kHF)>(
+          c.tile, src, [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); }, g,
+          t);
       tr.mark(2);
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
       tr.mark(3);
       const float* cbp = pr->cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
       float* gd = pr->gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
-      mid_columns<SPLIT, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
+      mid_columns<SPLIT, 3, hints(kHF, kHL, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
         const float rc = frcp(in[0]);
         const float q2 = y * rc;
-        __stcg(gd + idx, in[1] + q2);
+        stg1<kHL>(gd + idx, in[1] + q2);
         return -in[2] * q2 * rc;
       }, s > 1);
       tr.mark(4);
@@ -565,12 +670,12 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         float* vout = pr->v + pk * N;
         float* nout = pr->nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[1] = {php};
-        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
+        epi_rows_red<1, hints(kHN), kHL>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
           const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
                                         fdiv(y.w, in[0][3]));
-          st4(vout + idx, vv, nv, g.vec);
+          st4<kHL>(vout + idx, vv, nv, g.vec);
           return vv;
-        });
+        }, rot);
         tr.mark(6);
       }
     } else {  // ---------------- reverse pass, weight recursion
@@ -578,7 +683,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       const float* src[3] = {pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N, pr->r + pk * N,
                              pr->phi + slot(s) * PKN + pk * N};
       double dacc = 0;
-      stage_rows<SPLIT, 3>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
+      stage_rows<SPLIT, 3, hints(kHL, kHL, kHF)>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
         dacc += (double)__logf(v[2]) * (double)v[0];
         return fdiv(lam * v[0] - v[1], v[2]);
       }, g, t);
@@ -590,7 +695,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         tr.mark(3);
         const float* cbp = pr->cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
-        mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
+        mid_columns<SPLIT, 2, hints(kHF, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
           return y * (-in[1] * rc * rc);
         }, true);
@@ -602,14 +707,14 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         float* rout = pr->r + pk * N;
         float* gout = pr->gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
         const float* esrc[2] = {accp, php};
-        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
+        epi_rows_red<2, hints(kHN, kHN), kHL>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
           const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
                                         y.y * fdiv(__expf(in[0][1]), in[1][1]),
                                         y.z * fdiv(__expf(in[0][2]), in[1][2]),
                                         y.w * fdiv(__expf(in[0][3]), in[1][3]));
-          st4(rout + idx, rr, nv, g.vec);
+          st4<kHL>(rout + idx, rr, nv, g.vec);
           return rr;
-        });
+        }, rot);
         tr.mark(6);
       }
     }
@@ -668,8 +773,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
             const float q2 = bv / o32;
             gg = q2 > 0.f ? logf(q2) : (float)kLogEpsilon;
           }
-          if (dic) __stcg(n0 + j, gg);
-          __stcg(g0 + j, gg * bv);
+          if (dic) stg1<kHL>(n0 + j, gg);
+          stg1<kHL>(g0 + j, gg * bv);
         }
         const double tot = st_sum(lacc, s_dbl, st, t);
         if (t == 0) pr->loss[p] = lt == WDL_LOSS_TV ? 0.5 * tot : tot;
@@ -687,8 +792,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         float* zg = pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N;
         const bool dic = pr->need_dic != 0;
         for (size_t j = t; j < N; j += kSt) {
-          if (dic) __stcg(zn + j, 0.f);
-          __stcg(zg + j, 0.f);
+          if (dic) stg1<kHL>(zn + j, 0.f);
+          stg1<kHL>(zg + j, 0.f);
         }
       }
       bar_sync(st, kSt);
@@ -782,6 +887,7 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
   const long long streams = (a.total + 1) / 2;
   const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
   a.trace = nullptr;
+  a.dep_wait_ns = ctx->wait_limit_s > 0 ? (unsigned long long)(ctx->wait_limit_s * 1e9) : kDepWaitNs;
   if (ctx->trace_level >= 2) {
     if (!ctx->d_trace) WDL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_trace, 27 * sizeof(unsigned long long)));
     WDL_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_trace, 0, 27 * sizeof(unsigned long long), s));

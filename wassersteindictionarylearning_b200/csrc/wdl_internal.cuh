@@ -74,11 +74,17 @@ struct wdl_ctx {
 
   wdl::Arena arena;  // compute workspace (tape, scratch)
   wdl::Arena io;     // staging of the host-pointer calls
+  wdl::Arena lbfgs_arena;  // device L-BFGS state of wdl_regress_both (regress.cu)
   wdl::TcResources* tc = nullptr;
   int* fused_sync = nullptr;  // status block of the last fused-kernel launch (in the arena)
   // Device address of the library's fixed no-allocation scratch array on this
   // context's device, looked up when the context is created (noalloc.cu).
   void* noalloc_scratch = nullptr;
+  // Bound on one dependency wait of the fused kernel in seconds (0: the
+  // default), and a host-side fault to inject into the next batched launch
+  // (wdl_set_wait_limit, wdl_inject_fault).
+  double wait_limit_s = 0;
+  int inject_fault = 0;
 
   std::string last_error;
   long long launches = 0;
@@ -200,6 +206,11 @@ void tc_free(wdl_ctx* ctx);
 // Reads and clears the status word the tensor-core kernels set when a bounded
 // wait gives up (WDL_ERR_TIMEOUT); WDL_OK otherwise.
 int tc_check_status(wdl_ctx* ctx);
+// regress_both with the L-BFGS on the device (regress.cu); solution and
+// observed are device pointers.
+int regress_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, double scale_dic, double* solution,
+                     const double* observed, int max_iterations, double epsilon, int warm_restart,
+                     int* status, double* f_out, int* evaluations, cudaStream_t s);
 bool tc_supported(const wdl_ctx* ctx);
 // The context has the fused Sinkhorn kernel (tensor-core precision, 2-D, sides <= 128).
 bool tc_fused(const wdl_ctx* ctx);
@@ -241,6 +252,7 @@ struct SkArgs {
   double apps;                // operator applications the items perform (for profiling)
   int* sync;                  // work counter, error word
   unsigned long long* trace;  // [3 item types][8 phases + 1 count] ns, or null
+  unsigned long long dep_wait_ns;  // bound on one dependency wait
 };
 // Host helpers of the fused launch.
 void sk_fill_geometry(SkProblem& pr, int W, int H, bool split_bf16);

@@ -49,13 +49,18 @@ Evaluate = Callable[[np.ndarray, float], tuple]        # (x, step) -> (f, g)
 Progress = Callable[[np.ndarray, np.ndarray, float, float, float, float, int, int], int]
 
 
-def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
-    """Resumable form: a generator that yields each point to evaluate and
+def _minimize(x0: np.ndarray, p: LbfgsParam, progress: Optional[Progress], nan_cancel: bool,
+              state: dict):
+    """The algorithm, once: a generator that yields each point to evaluate and
     receives (f, g) through send(); it returns (status, x, f) via StopIteration.
-    Same algorithm and constants as lbfgs() below (which drives it)."""
-    p = param or LbfgsParam()
+    state["step"] holds the line-search step of the point being evaluated (0
+    for the first evaluation).  progress, when given, is called after every
+    accepted step (lbfgs.c:522-529) and a non-zero return stops the run; with
+    nan_cancel a NaN objective stops it instead (LBFGSERR_CANCELED, the
+    reference's progress_both, cpp/inverseWasserstein.h:1180-1184)."""
     x = np.array(x0, dtype=np.float64, copy=True)
     n = x.size
+    state["step"] = 0.0
     f, g = yield x
     g = np.asarray(g, dtype=np.float64)
     d = -g
@@ -68,10 +73,14 @@ def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
     y_hist = np.zeros((p.m, n))
     ys_hist = np.zeros(p.m)
     alpha = np.zeros(p.m)
+    pf = np.zeros(max(p.past, 1))
+    if p.past > 0:
+        pf[0] = f
     k, end = 1, 0
     while True:
         xp, gp = x.copy(), g.copy()
-        # backtracking line search with the strong Wolfe test (lbfgs.c:772-867)
+        # backtracking line search with the strong Wolfe test (lbfgs.c:772-867);
+        # on failure the run stops at the previous point (lbfgs.c:487-492)
         if step <= 0:
             return LBFGSERR_INVALIDPARAMETERS, xp, f
         dginit = float(np.dot(g, d))
@@ -80,6 +89,7 @@ def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
         finit, dgtest, count = f, p.ftol * dginit, 0
         while True:
             x = xp + step * d
+            state["step"] = step
             f, g = yield x
             g = np.asarray(g, dtype=np.float64)
             count += 1
@@ -102,100 +112,12 @@ def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
             step *= width
         xnorm = float(np.linalg.norm(x))
         gnorm = float(np.linalg.norm(g))
-        if np.isnan(f):
-            return LBFGSERR_CANCELED, x, f
-        if gnorm / max(xnorm, 1.0) <= p.epsilon:
-            return LBFGS_SUCCESS, x, f
-        if p.max_iterations != 0 and p.max_iterations < k + 1:
-            return LBFGSERR_MAXIMUMITERATION, x, f
-        s_hist[end] = x - xp
-        y_hist[end] = g - gp
-        ys = float(np.dot(y_hist[end], s_hist[end]))
-        yy = float(np.dot(y_hist[end], y_hist[end]))
-        ys_hist[end] = ys
-        bound = min(p.m, k)
-        k += 1
-        end = (end + 1) % p.m
-        d = -g
-        j = end
-        for _ in range(bound):
-            j = (j + p.m - 1) % p.m
-            alpha[j] = float(np.dot(s_hist[j], d)) / ys_hist[j]
-            d = d - alpha[j] * y_hist[j]
-        d = d * (ys / yy)
-        for _ in range(bound):
-            beta = float(np.dot(y_hist[j], d)) / ys_hist[j]
-            d = d + (alpha[j] - beta) * s_hist[j]
-            j = (j + 1) % p.m
-        step = 1.0
-
-
-def _line_search(x, f, g, d, step, xp, evaluate, p: LbfgsParam):
-    """Backtracking with the strong Wolfe conditions; returns (count or code, x, f, g, step)."""
-    count = 0
-    if step <= 0:
-        return LBFGSERR_INVALIDPARAMETERS, x, f, g, step
-    dginit = float(np.dot(g, d))
-    if dginit > 0:
-        return LBFGSERR_INCREASEGRADIENT, x, f, g, step
-    finit = f
-    dgtest = p.ftol * dginit
-    while True:
-        x = xp + step * d
-        f, g = evaluate(x, step)
-        count += 1
-        if f > finit + step * dgtest:
-            width = 0.5
-        else:
-            dg = float(np.dot(g, d))
-            if dg < p.wolfe * dginit:
-                width = 2.1
-            elif dg > -p.wolfe * dginit:
-                width = 0.5
-            else:
-                return count, x, f, g, step
-        if step < p.min_step:
-            return LBFGSERR_MINIMUMSTEP, x, f, g, step
-        if step > p.max_step:
-            return LBFGSERR_MAXIMUMSTEP, x, f, g, step
-        if p.max_linesearch <= count:
-            return LBFGSERR_MAXIMUMLINESEARCH, x, f, g, step
-        step *= width
-
-
-def lbfgs(x0: np.ndarray, evaluate: Evaluate, progress: Optional[Progress] = None,
-          param: Optional[LbfgsParam] = None):
-    """Minimise f from x0.  Returns (status, x, f)."""
-    p = param or LbfgsParam()
-    x = np.array(x0, dtype=np.float64, copy=True)
-    n = x.size
-    f, g = evaluate(x, 0.0)
-    g = np.asarray(g, dtype=np.float64)
-    d = -g
-    xnorm = max(float(np.linalg.norm(x)), 1.0)
-    gnorm = float(np.linalg.norm(g))
-    if gnorm / xnorm <= p.epsilon:
-        return LBFGS_ALREADY_MINIMIZED, x, f
-    step = 1.0 / float(np.sqrt(np.dot(d, d)))
-    s_hist = np.zeros((p.m, n))
-    y_hist = np.zeros((p.m, n))
-    ys_hist = np.zeros(p.m)
-    alpha = np.zeros(p.m)
-    pf = np.zeros(max(p.past, 1))
-    if p.past > 0:
-        pf[0] = f
-    k, end = 1, 0
-    while True:
-        xp, gp = x.copy(), g.copy()
-        ls, x, f, g, step = _line_search(x, f, g, d, step, xp, evaluate, p)
-        if ls < 0:  # revert to the previous point (lbfgs.c:487-492)
-            return ls, xp, f
-        xnorm = float(np.linalg.norm(x))
-        gnorm = float(np.linalg.norm(g))
         if progress is not None:
-            ret = progress(x, g, f, xnorm, gnorm, step, k, ls)
+            ret = progress(x, g, f, xnorm, gnorm, step, k, count)
             if ret:
                 return ret, x, f
+        if nan_cancel and np.isnan(f):
+            return LBFGSERR_CANCELED, x, f
         if gnorm / max(xnorm, 1.0) <= p.epsilon:
             return LBFGS_SUCCESS, x, f
         if p.past > 0:
@@ -206,6 +128,7 @@ def lbfgs(x0: np.ndarray, evaluate: Evaluate, progress: Optional[Progress] = Non
             pf[k % p.past] = f
         if p.max_iterations != 0 and p.max_iterations < k + 1:
             return LBFGSERR_MAXIMUMITERATION, x, f
+        # two-loop recursion over the m most recent pairs (lbfgs.c:570-612)
         s_hist[end] = x - xp
         y_hist[end] = g - gp
         ys = float(np.dot(y_hist[end], s_hist[end]))
@@ -226,3 +149,24 @@ def lbfgs(x0: np.ndarray, evaluate: Evaluate, progress: Optional[Progress] = Non
             d = d + (alpha[j] - beta) * s_hist[j]
             j = (j + 1) % p.m
         step = 1.0
+
+
+def lbfgs_steps(x0: np.ndarray, param: Optional[LbfgsParam] = None):
+    """Resumable form: a generator that yields each point to evaluate and
+    receives (f, g) through send(); it returns (status, x, f) via StopIteration.
+    A NaN objective cancels the run as the reference's progress_both does."""
+    return _minimize(x0, param or LbfgsParam(), None, True, {})
+
+
+def lbfgs(x0: np.ndarray, evaluate: Evaluate, progress: Optional[Progress] = None,
+          param: Optional[LbfgsParam] = None):
+    """Minimise f from x0 with evaluate(x, step) -> (f, g) and the optional
+    progress callback (liblbfgs' lbfgs(), lbfgs.c:256-654).  Returns (status, x, f)."""
+    state = {}
+    gen = _minimize(x0, param or LbfgsParam(), progress, False, state)
+    try:
+        x = next(gen)
+        while True:
+            x = gen.send(evaluate(x, state["step"]))
+    except StopIteration as stop:
+        return stop.value

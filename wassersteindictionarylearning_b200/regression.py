@@ -9,6 +9,7 @@ histograms, and ``regress_both`` (:362-521) drives it with the host L-BFGS of
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from typing import Optional
 
@@ -142,6 +143,24 @@ class WassersteinRegression:
         if math.isnan(fx):  # :1180-1184
             return _lb.LBFGSERR_CANCELED
         return 0
+
+    def regress_both_device(self, solution: np.ndarray) -> int:
+        """regress_both with the L-BFGS on the device (wdl_regress_both): the
+        same optimisation, no per-evaluation host round trip of the n-vectors.
+        Optimises ``solution`` (original domain) in place; returns liblbfgs'
+        status of the last run."""
+        P, K, N = self.P, self.K, self.N
+        sol = f64(solution)
+        status, fval, evals = C.c_int(), C.c_double(), C.c_int()
+        ctx = self.problem.kernel.ctx
+        check(lib().wdl_regress_both(ctx, P, K, self.Niters, self.loss_type, self.scaleDictionary,
+                                     dptr(sol), dptr(self.problem.observed_pdf), int(self.wrTotalIteration),
+                                     float(self.lbfgs_param.epsilon), int(bool(self.warmRestart)),
+                                     C.byref(status), C.byref(fval), C.byref(evals)), ctx)
+        solution[:] = sol
+        self.device_evaluations = evals.value
+        self.device_objective = fval.value
+        return status.value
 
     def regress_both(self, solution: np.ndarray) -> int:
         """Optimise [weights, atoms] in place (original domain on entry and exit)."""
