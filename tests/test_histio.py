@@ -103,7 +103,9 @@ def test_exporters(tmp_path):
     names = ["h0", "h1"]
     d = str(tmp_path)
     assert hio.ExportHistogramToCSV(d, digits=17).exportHistogramsBatch(hists, names) == 0
-    assert np.array_equal(hio.load_csv_to_pdf(os.path.join(d, "h0.csv"))[0], hists[0] / hists[0].sum())
+    # the reference's reader takes the last value twice when the file ends with a newline
+    h = np.append(hists[0], hists[0][-1])
+    assert np.array_equal(hio.load_csv_to_pdf(os.path.join(d, "h0.csv"))[0], h / h.sum())
     assert hio.ExportHistogramToCSV(d).exportHistogram(np.array([1.0 / 3, 12345678.0]), "g") == 0
     assert open(os.path.join(d, "g.csv")).read() == "0.333333\n1.23457e+07\n"
     assert hio.ExportHistogramToRAW(d).exportHistogramsBatch(hists, names) == 0
@@ -111,9 +113,68 @@ def test_exporters(tmp_path):
     assert hio.ExportHistogramToImage(12, 10, d).exportHistogram(hists[0], "i0") == 0
     im = hio.read_image(os.path.join(d, "i0.png"))
     q = hio.quantile(hists[0], [0.95])[0]
-    assert np.array_equal(im, np.clip(hists[0].reshape(10, 12) * 255 * 0.95 / q, 0, 255).astype(np.uint8))
+    assert im.shape == (10, 12, 3) and (im == im[:, :, :1]).all()  # grey in three channels
+    assert np.array_equal(im[:, :, 0], np.clip(hists[0].reshape(10, 12) * 255 * 0.95 / q, 0, 255).astype(np.uint8))
     ex = hio.ExportHistogramToImageWithScaling(12, 10, [2.0, 3.0], d, alpha=1.0, complement=True)
     assert ex.exportHistogramsBatch(hists, names) == 0
-    im1 = hio.read_image(os.path.join(d, "h1.png"))
+    im1 = hio.read_image(os.path.join(d, "h1.png"))[:, :, 0]
     assert np.array_equal(im1, np.clip(255 - hists[1].reshape(10, 12) * 3.0 * 255, 0, 255).astype(np.uint8))
     assert hio.ExportHistogramToCSV(d).exportHistogramsBatch(hists, ["x"]) == -1
+
+
+# ---- against the reference's own loaders and exporters (golden histio_ref) ----------
+def _ref_fixture():
+    from conftest import golden
+    (_, f), = golden("histio_ref")
+    return f
+
+
+def _write(tmp_path, name, arr):
+    p = str(tmp_path / name)
+    open(p, "wb").write(bytes(arr))
+    return p
+
+
+def test_loaders_match_reference_cimg(tmp_path):
+    """load_img_to_pdf / _grayscale_luma / _gamma_correction / load_csv_to_pdf on the
+    PGM / PPM / CSV files the reference read through CImg (cpp/histogramIO.h:243-337)."""
+    from wassersteindictionarylearning_b200 import histio
+    f = _ref_fixture()
+    W, H = int(f["W"]), int(f["H"])
+    pgm = _write(tmp_path, "a.pgm", f["pgm"])
+    ppm = _write(tmp_path, "a.ppm", f["ppm"])
+    csv = _write(tmp_path, "a.csv", f["csv"])
+    pdf, w, h, s = histio.load_img_to_pdf(pgm)
+    assert (w, h) == (W, H)
+    assert np.allclose(pdf, f["pdf_gray"], rtol=1e-14, atol=0) and abs(s - float(f["sum_gray"])) < 1e-9
+    pdf, _, _, s = histio.load_img_to_pdf(ppm)  # first channel of an RGB file
+    assert np.allclose(pdf, f["pdf_ppm_first"], rtol=1e-14, atol=0)
+    pdf, _, _, s = histio.load_rgb_img_to_pdf_grayscale_luma(ppm)
+    assert np.allclose(pdf, f["pdf_luma"], rtol=1e-14, atol=0) and abs(s / float(f["sum_luma"]) - 1) < 1e-14
+    for alpha, comp in ((0.5, 0), (2.2, 1)):
+        pdf, _, _, s = histio.load_img_to_pdf_gamma_correction(pgm, alpha, bool(comp))
+        assert np.allclose(pdf, f[f"pdf_gamma_{alpha}_{comp}"], rtol=1e-13, atol=0)
+        assert abs(s / float(f[f"sum_gamma_{alpha}_{comp}"]) - 1) < 1e-13
+    pdf, s = histio.load_csv_to_pdf(csv)
+    assert np.allclose(pdf, f["pdf_csv"], rtol=1e-15, atol=0)
+
+
+def test_exporters_write_the_reference_bytes(tmp_path):
+    """save_pdf / save_pdf_gamma_correction write the same PNM file as the reference
+    (three replicated channels, truncation to unsigned char, cpp/histogramIO.h:339-371)."""
+    from wassersteindictionarylearning_b200 import histio
+    f = _ref_fixture()
+    W, H = int(f["W"]), int(f["H"])
+    val = f["pdf_gray"]
+    p1, p2 = str(tmp_path / "o1.ppm"), str(tmp_path / "o2.ppm")
+    histio.save_pdf(p1, W, H, val, float(f["save_pdf_scaling"]))
+    assert open(p1, "rb").read() == bytes(f["save_pdf_bytes"])
+    histio.save_pdf_gamma_correction(p2, W, H, val, 2.2, True, float(f["save_gamma_scaling"]))
+    assert open(p2, "rb").read() == bytes(f["save_gamma_bytes"])
+
+
+def test_quantile_matches_reference():
+    from wassersteindictionarylearning_b200 import histio
+    f = _ref_fixture()
+    q = histio.quantile(f["quantile_data"], list(f["quantile_probs"]))
+    assert np.allclose(q, f["quantile"], rtol=1e-15, atol=0)

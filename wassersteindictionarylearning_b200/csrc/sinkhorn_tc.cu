@@ -207,7 +207,11 @@ template <bool SPLIT, int NIN, uint32_t HS = 0, class F>
 __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
                                            F f, const Geo& g, int t) {
   constexpr int CE = SPLIT ? 8 : 4;
+#ifndef WDL_X_UNR
   constexpr int UNR = NIN > 2 ? 1 : 2;
+#else
+  constexpr int UNR = NIN > 2 ? WDL_X_UNR : 2;
+#endif
   const int total = g.Hp * (int)g.cpr;
   for (int base = t; base < total; base += kSt * UNR) {
     float in[UNR][NIN > 0 ? NIN : 1][CE];
@@ -387,7 +391,11 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
   bar_sync(c.st, kSt);
   const int j = c.t & 31;  // 16-byte chunk of the row
   const int x0 = 4 * j;
+#ifndef WDL_X_U
   constexpr int U = 2;
+#else
+  constexpr int U = WDL_X_U;
+#endif
   for (int i0 = c.t >> 5; i0 < g.H; i0 += kWarps * U) {
     float4 y4[U];
     float in[U][NIN > 0 ? NIN : 1][4];
@@ -485,11 +493,16 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   SkProblem* const pr = &s_prob[st];
   int cur_q = -1;
   Trace tr;
+#ifndef WDL_X_EARLY
+#define WDL_X_EARLY 0
+#endif
+  int next_item = -1;  // thread 0: the item claimed during the previous completion
   while (true) {
     tr.start(a.trace, t);
     tr.type = 0;
     if (t == 0) {
-      const int item = atomicAdd(work, 1);
+      const int item = next_item >= 0 ? next_item : atomicAdd(work, 1);
+      next_item = -1;
       int q = 0, type = 0, step = 0, pkv = 0;
       if (item < a.total) {
         if (a.items) {
@@ -726,6 +739,9 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     // Completion: the item that finishes a group publishes it.
     bar_sync(st, kSt);
     if (t == 0) {
+      // the next item's claim goes out before this item's release fence, so
+      // its round trip overlaps the fence and the completion count
+      if (WDL_X_EARLY) next_item = atomicAdd(work, 1);
       __threadfence();
       int fin;
       if (type == 0) fin = atomicAdd(&done_fwd[p], 1) + 1 == step * K;

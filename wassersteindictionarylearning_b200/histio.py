@@ -207,7 +207,30 @@ def load_img_to_pdf_gamma_correction(path: str, alpha: float, complement: bool):
 
 
 def load_csv_to_pdf(path: str):
-    v = np.array([float(t) for t in open(path).read().split()], dtype=np.float64)
+    """(pdf, sum) as the reference's loop `while (ifs.good()) { ifs >> v; sum += v;
+    result.push_back(v); }` (cpp/histogramIO.h:314-337) reads it: when the file
+    ends with whitespace the extraction after the last value fails before
+    touching v, so the last value is appended (and summed) a second time; a
+    token that is not a number stores 0 and ends the loop."""
+    text = open(path).read()
+    vals = []
+    failed = False
+    for tok in text.split():
+        try:
+            v = float(tok)
+            if not np.isfinite(v) and tok.lower().lstrip("+-") in ("nan", "inf", "infinity"):
+                raise ValueError(tok)  # iostream does not parse these words
+        except ValueError:
+            failed = True
+            break
+        vals.append(v)
+    if failed:
+        vals.append(0.0)
+    elif not vals:
+        raise ValueError(f"{path}: no values (the reference reads an uninitialised value here)")
+    elif text[-1:].isspace():
+        vals.append(vals[-1])
+    v = np.array(vals, dtype=np.float64)
     s = float(v.sum())
     return v / s, s
 
@@ -221,14 +244,20 @@ def _to_u8(v: np.ndarray) -> np.ndarray:
     return np.clip(v, 0.0, 255.0).astype(np.uint8)
 
 
+def _rgb(gray: np.ndarray) -> np.ndarray:
+    # the reference replicates the grey plane into three channels before saving
+    # (cpp/histogramIO.h:341-347), so its files are RGB
+    return np.repeat(gray[:, :, None], 3, axis=2)
+
+
 def save_pdf(path: str, W: int, H: int, val, scaling: float) -> None:
-    write_image(path, _to_u8(np.asarray(val, dtype=np.float64).reshape(H, W) * scaling))
+    write_image(path, _rgb(_to_u8(np.asarray(val, dtype=np.float64).reshape(H, W) * scaling)))
 
 
 def save_pdf_gamma_correction(path: str, W: int, H: int, val, alpha: float, complement: bool,
                               scaling: float) -> None:
     g = np.power(np.asarray(val, dtype=np.float64).reshape(H, W) * scaling, 1.0 / alpha) * 255.0
-    write_image(path, _to_u8(255.0 - g if complement else g))
+    write_image(path, _rgb(_to_u8(255.0 - g if complement else g)))
 
 
 def quantile(data, probs):
