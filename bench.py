@@ -84,7 +84,7 @@ def parse():
     ap.add_argument("--no-arms", action="store_true")
     ap.add_argument("--no-regress", action="store_true")
     ap.add_argument("--regress-iters", type=int, default=3)
-    ap.add_argument("--serve-rates", default="50,200,500,2000")
+    ap.add_argument("--serve-rates", default="8,50,200,500,2000")
     ap.add_argument("--serve-requests", type=int, default=120)
     # Reduced sizes for profiler captures (the bench line itself uses the workload's).
     ap.add_argument("--P", type=int, default=None)
@@ -343,7 +343,8 @@ def run_ours(args):
                                   tile_rows=choice.value, ms=round(tms.value, 4)))
             else:  # log-domain axis pass: rows per block
                 tuned.append(dict(kind="log_axis_pass", rows=key6[1], row_len=key6[2], images=key6[3],
-                                  signed=bool(key6[5]), rows_per_block=choice.value,
+                                  signed=bool(key6[5]), rows_per_block=choice.value % 100,
+                                  layout="warp per row" if choice.value >= 100 else "rows fastest",
                                   ms=round(tms.value, 4)))
     peaks = {}
     try:

@@ -85,6 +85,9 @@ int build_factors(wdl_ctx* ctx) {
     // expanded to the dense symmetric factor G[i][j] = kernel1d[|i-j|].
     std::vector<double> k1d(n);
     for (int i = 0; i < n; ++i) k1d[i] = std::max(kEpsilon, std::exp(-(i * i) / ctx->gamma));
+    ctx->axis_reach[a] = 0;
+    for (int i = 0; i < n; ++i)
+      if ((float)k1d[i] != 0.f) ctx->axis_reach[a] = i;
     for (int i = 0; i < n; ++i)
       for (int j = 0; j < n; ++j) {
         g64[(size_t)i * n + j] = k1d[std::abs(i - j)];

@@ -165,24 +165,72 @@ struct LogOps<double> {
   __device__ static double lg(double x) { return log(x); }
 };
 
-template <typename T, bool SIGNED, int LR>
-__global__ void __launch_bounds__(256) log_axis_pass_kernel(
-    const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
-    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
-    unsigned long long* __restrict__ exps) {
+// One output of the log-domain pass: out = log |sum_k s_k exp(lk[|c-k|] + row[k])|
+// (in the kernel's base) and its sign, by the two passes described above.  Both
+// kernel layouts below call this, so an output's arithmetic does not depend on
+// the layout.  *taps receives the number of exponentials evaluated.
+template <typename T, bool SIGNED>
+__device__ __forceinline__ T log_out(const T* __restrict__ row, const uint8_t* __restrict__ sgn,
+                                     const T* __restrict__ lk, T X, int c, int C, bool* pos, unsigned* taps) {
   using Op = LogOps<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int CP = C + 1;                                 // odd row stride (elements)
-  T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
-  T* lk = rows + LR * CP;                               // [C]: -d^2/gamma (scaled)
-  T* xmax = lk + C;                                     // [LR]
-  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);  // [LR][C + 4] (bank-spread bytes)
-  const int SP = C + 4;
-  const int r0 = blockIdx.x * LR;
-  const size_t base = (size_t)blockIdx.y * img_stride;
-  const int nr = min(LR, R - r0);
+  const int dboth = min(c, C - 1 - c);      // both sides inside the row for d <= dboth
+  const int sgnd = c < C - 1 - c ? 1 : -1;  // the side that remains beyond dboth
+  T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
+  int d = 1;
+  for (; d <= dboth; ++d) {
+    const T l = lk[d];
+    if (l + X <= m) break;
+    const T a = l + row[c - d], b = l + row[c + d];
+    const T ab = a > b ? a : b;
+    m = ab > m ? ab : m;
+  }
+  if (d > dboth) {
+    for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
+      const T l = lk[d];
+      if (l + X <= m) break;
+      const T t = l + row[c + sgnd * d];
+      m = t > m ? t : m;
+    }
+  }
+  T sum = Op::ex(row[c] - m);
+  if (SIGNED && !sgn[c]) sum = -sum;
+  const T fl = m - Op::kTail;
+  for (d = 1; d <= dboth; ++d) {
+    const T l = lk[d];
+    if (l + X < fl) break;
+    const T lm = l - m;
+    const T ea = Op::ex(lm + row[c - d]), eb = Op::ex(lm + row[c + d]);
+    if (SIGNED) sum += (sgn[c - d] ? ea : -ea) + (sgn[c + d] ? eb : -eb);
+    else sum += ea + eb;
+  }
+  if (d > dboth) {
+    for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
+      const T l = lk[d];
+      if (l + X < fl) break;
+      const int k = c + sgnd * d;
+      const T ex = Op::ex((l - m) + row[k]);
+      sum += (!SIGNED || sgn[k]) ? ex : -ex;
+    }
+  }
+  const int dmax = d - 1;  // the last tap distance summed
+  *taps += 1 + min(dmax, c) + min(dmax, C - 1 - c);
+  if (SIGNED) {
+    *pos = sum >= T(0);
+    return (Op::lg(fabs(sum)) + m) * Op::kUnscale;
+  }
+  *pos = true;
+  return (Op::lg(sum) + m) * Op::kUnscale;
+}
+
+// Stage LR rows of one image in SMEM (odd row stride CP), their signs, the row
+// maxima X and the tap table lk[d] = -d^2/gamma (scaled).
+template <typename T, bool SIGNED, int LR>
+__device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_t* __restrict__ in_sign,
+                                          T* rows, uint8_t* sg, T* xmax, T* lk, size_t base, int r0, int nr,
+                                          int C, int CP, int SP, T gamma_t) {
+  using Op = LogOps<T>;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // stage: warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
+  // warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
   for (int rr = warp; rr < LR; rr += 8) {
     T vm = Op::kFloor;
     for (int k = lane; k < C; k += 32) {
@@ -204,63 +252,91 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     if (lane == 0) xmax[rr] = vm;
   }
   for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d) * T(d) / gamma_t * Op::kScale;
+}
+
+// Layout "rows fastest": a block owns LR rows of one image and thread e makes
+// output (c = e / LR, rr = e % LR), so the stores out[c][r0 + rr] of a warp are
+// contiguous runs.
+template <typename T, bool SIGNED, int LR>
+__global__ void __launch_bounds__(256) log_axis_pass_kernel(
+    const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
+    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
+    unsigned long long* __restrict__ exps) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int CP = C + 1;                                 // odd row stride (elements)
+  T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
+  T* lk = rows + LR * CP;                               // [C]: -d^2/gamma (scaled)
+  T* xmax = lk + C;                                     // [LR]
+  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);  // [LR][C + 4] (bank-spread bytes)
+  const int SP = C + 4;
+  const int r0 = blockIdx.x * LR;
+  const size_t base = (size_t)blockIdx.y * img_stride;
+  const int nr = min(LR, R - r0);
+  const int lane = threadIdx.x & 31;
+  log_stage<T, SIGNED, LR>(in, in_sign, rows, sg, xmax, lk, base, r0, nr, C, CP, SP, gamma_t);
   __syncthreads();
-  // Thread -> (c, rr) with rr fastest so that stores out[c][r0+rr] are contiguous.
   unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
   for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
     const int c = e / LR, rr = e - c * LR;
     if (rr >= nr) continue;
-    const T* row = rows + rr * CP;
-    const T X = xmax[rr];
-    const int dboth = min(c, C - 1 - c);  // both sides inside the row for d <= dboth
-    const int sgnd = c < C - 1 - c ? 1 : -1;  // the side that remains beyond dboth
-    T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
-    int d = 1;
-    for (; d <= dboth; ++d) {
-      const T l = lk[d];
-      if (l + X <= m) break;
-      const T a = l + row[c - d], b = l + row[c + d];
-      const T ab = a > b ? a : b;
-      m = ab > m ? ab : m;
-    }
-    if (d > dboth) {
-      for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
-        const T l = lk[d];
-        if (l + X <= m) break;
-        const T t = l + row[c + sgnd * d];
-        m = t > m ? t : m;
-      }
-    }
-    const uint8_t* sgn = sg + rr * SP;
-    T sum = Op::ex(row[c] - m);
-    if (SIGNED && !sgn[c]) sum = -sum;
-    const T fl = m - Op::kTail;
-    for (d = 1; d <= dboth; ++d) {
-      const T l = lk[d];
-      if (l + X < fl) break;
-      const T lm = l - m;
-      const T ea = Op::ex(lm + row[c - d]), eb = Op::ex(lm + row[c + d]);
-      if (SIGNED) sum += (sgn[c - d] ? ea : -ea) + (sgn[c + d] ? eb : -eb);
-      else sum += ea + eb;
-    }
-    if (d > dboth) {
-      for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
-        const T l = lk[d];
-        if (l + X < fl) break;
-        const int k = c + sgnd * d;
-        const T ex = Op::ex((l - m) + row[k]);
-        sum += (!SIGNED || sgn[k]) ? ex : -ex;
-      }
-    }
+    bool pos;
+    const T v = log_out<T, SIGNED>(rows + rr * CP, sg + rr * SP, lk, xmax[rr], c, C, &pos, &n_ex);
     const size_t o = base + (size_t)c * R + (r0 + rr);
-    if (SIGNED) {
-      out_sign[o] = sum >= T(0) ? 1 : 0;
-      out[o] = (Op::lg(fabs(sum)) + m) * Op::kUnscale;
-    } else {
-      out[o] = (Op::lg(sum) + m) * Op::kUnscale;
+    out[o] = v;
+    if (SIGNED) out_sign[o] = pos ? 1 : 0;
+  }
+  if (exps) {
+    unsigned long long v = n_ex;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(exps, v);
+  }
+}
+
+// Layout "row per warp": warp w makes the outputs of rows w, w + 8, ..., its
+// lanes taking 32 consecutive c of one row, so the lanes of a warp run nearly
+// the same number of taps (neighbouring outputs of one row) and read
+// consecutive SMEM words; the results go through SMEM ([C][LR + 1]) and are
+// stored as contiguous runs of out[c][r0..].  Same outputs, bit for bit, as
+// the layout above.
+template <typename T, bool SIGNED, int LR>
+__global__ void __launch_bounds__(256) log_axis_pass_rowwarp_kernel(
+    const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
+    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
+    unsigned long long* __restrict__ exps) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int CP = C + 1;
+  T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
+  T* lk = rows + LR * CP;                               // [C]
+  T* xmax = lk + C;                                     // [LR]
+  T* ot = xmax + LR;                                    // [C][LR + 1] results
+  uint8_t* sg = reinterpret_cast<uint8_t*>(ot + (size_t)C * (LR + 1));  // [LR][C + 4]
+  const int SP = C + 4;
+  uint8_t* osg = sg + LR * SP;                          // [C][LR + 1] result signs
+  const int r0 = blockIdx.x * LR;
+  const size_t base = (size_t)blockIdx.y * img_stride;
+  const int nr = min(LR, R - r0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  log_stage<T, SIGNED, LR>(in, in_sign, rows, sg, xmax, lk, base, r0, nr, C, CP, SP, gamma_t);
+  __syncthreads();
+  unsigned n_ex = 0;
+  for (int rr = warp; rr < nr; rr += 8) {
+    const T* row = rows + rr * CP;
+    const uint8_t* sgn = sg + rr * SP;
+    const T X = xmax[rr];
+    for (int c = lane; c < C; c += 32) {
+      bool pos;
+      ot[(size_t)c * (LR + 1) + rr] = log_out<T, SIGNED>(row, sgn, lk, X, c, C, &pos, &n_ex);
+      if (SIGNED) osg[(size_t)c * (LR + 1) + rr] = pos ? 1 : 0;
     }
-    const int dmax = d - 1;  // the last tap distance summed
-    n_ex += 1 + min(dmax, c) + min(dmax, C - 1 - c);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
+    const int c = e / LR, rr = e - c * LR;
+    if (rr >= nr) continue;
+    const size_t o = base + (size_t)c * R + (r0 + rr);
+    out[o] = ot[(size_t)c * (LR + 1) + rr];
+    if (SIGNED) out_sign[o] = osg[(size_t)c * (LR + 1) + rr];
   }
   if (exps) {
     unsigned long long v = n_ex;
@@ -271,14 +347,16 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
 }
 
 template <typename T>
-size_t log_axis_smem(int LR, int C) {
-  return ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
+size_t log_axis_smem(int LR, int C, bool rowwarp = false) {
+  size_t b = ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
+  if (rowwarp) b += (size_t)C * (LR + 1) * (sizeof(T) + 1);
+  return b;
 }
 
-template <typename T, int LR>
+template <typename T, int LR, bool ROWWARP>
 int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
                     const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
-  const size_t smem = log_axis_smem<T>(LR, C);
+  const size_t smem = log_axis_smem<T>(LR, C, ROWWARP);
   const T gamma_t = T(ctx->gamma);
   size_t done = 0;
   while (done < nimg) {
@@ -287,12 +365,12 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
     dim3 grid((R + LR - 1) / LR, (unsigned)chunk);
     size_t off = done * img_stride;
     if (in_sign) {
-      auto k = log_axis_pass_kernel<T, true, LR>;
+      auto k = ROWWARP ? log_axis_pass_rowwarp_kernel<T, true, LR> : log_axis_pass_kernel<T, true, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
                                 out_sign + off, ctx->profiling ? ctx->d_taps : nullptr);
     } else {
-      auto k = log_axis_pass_kernel<T, false, LR>;
+      auto k = ROWWARP ? log_axis_pass_rowwarp_kernel<T, false, LR> : log_axis_pass_kernel<T, false, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr,
                                 ctx->profiling ? ctx->d_taps : nullptr);
@@ -307,10 +385,14 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
 template <typename T>
 int log_axis_dispatch(wdl_ctx* ctx, int LR, const T* in, T* out, int R, int C, size_t nimg,
                       size_t img_stride, const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+  // choice: rows per block (LR), plus 100 for the row-per-warp layout
   switch (LR) {
-    case 8: return log_axis_launch<T, 8>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 32: return log_axis_launch<T, 32>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    default: return log_axis_launch<T, 16>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 8: return log_axis_launch<T, 8, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 32: return log_axis_launch<T, 32, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 108: return log_axis_launch<T, 8, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 116: return log_axis_launch<T, 16, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 132: return log_axis_launch<T, 32, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    default: return log_axis_launch<T, 16, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
   }
 }
 
@@ -330,7 +412,7 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
   cudaStreamIsCapturing(s, &cap);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
     return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-  const int cand[3] = {8, 16, 32};
+  const int cand[6] = {8, 16, 32, 108, 116, 132};
   int best = kLogRowsDefault;
   float best_ms = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -338,7 +420,7 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
   int rc = WDL_OK;
   for (int c : cand) {
-    if (log_axis_smem<T>(c, C) > 200 * 1024) continue;
+    if (log_axis_smem<T>(c % 100, C, c >= 100) > 200 * 1024) continue;
     // an untimed run first: the first launch of a variant also loads it
     if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s))) break;
     cudaEventRecord(e0, s);

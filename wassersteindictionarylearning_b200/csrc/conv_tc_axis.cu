@@ -156,7 +156,7 @@ __global__ void k_build_factor_blocks(const float* __restrict__ G, int C, uint8_
 template <bool SPLIT, int TR>
 __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
     tc_axis_kernel(const float* __restrict__ in, float* __restrict__ out,
-                   const uint8_t* __restrict__ gblocks, int R, int C, size_t img_stride, int* err) {
+                   const uint8_t* __restrict__ gblocks, int R, int C, size_t img_stride, int reach, int* err) {
   using Ge = AxGeom<TR>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -167,6 +167,13 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
   const float* src = in + (size_t)blockIdx.z * img_stride + (size_t)r0 * C;
   const int nch = (C + kAxKc - 1) / kAxKc;
   const uint8_t* gsrc = gblocks + (size_t)blockIdx.x * nch * kAxOperand;
+  // K chunks whose factor rows c0.. are not all zero: |c - k| <= reach.  The
+  // other chunks' FP32 factor entries (hence their BF16 / TF32 operands) are
+  // exactly zero and add exactly nothing, so they are neither loaded nor
+  // multiplied.
+  const int c_last = min(c0 + kAxTile, C) - 1;
+  const int jlo = max(0, c0 - reach) / kAxKc;
+  const int jhi = min(C - 1, c_last + reach) / kAxKc + 1;
   float* dst = out + (size_t)blockIdx.z * img_stride;
   const int b_rows = min(TR, R - r0);
   const bool vec = (C & 3) == 0;
@@ -186,13 +193,14 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
   const uint32_t id = ptx::idesc(F::fmt, 128, TR);
   bool ok = true;
   OperandRegs<SPLIT, TR> breg;
-  load_operand<SPLIT, TR>(breg, src, b_rows, C, 0, vec, t);
-  for (int j = 0; j < nch; ++j) {
-    const int st = j & 1;
+  load_operand<SPLIT, TR>(breg, src, b_rows, C, jlo * kAxKc, vec, t);
+  for (int j = jlo; j < jhi; ++j) {
+    const int jj = j - jlo;  // position in this CTA's chunk sequence
+    const int st = jj & 1;
     uint8_t* a_tile = base + st * Ge::kStage;
     uint8_t* b_tile = a_tile + kAxOperand;
-    if (j >= 2) {  // the MMAs of chunk j-2 read this stage: wait for their commit
-      const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[st]), (uint32_t)(((j - 2) >> 1) & 1), kWaitNs);
+    if (jj >= 2) {  // the MMAs of chunk jj-2 read this stage: wait for their commit
+      const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[st]), (uint32_t)(((jj - 2) >> 1) & 1), kWaitNs);
       ok = __syncthreads_and(w) != 0;
       if (!ok) break;
     }
@@ -207,7 +215,7 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
       cp_async_commit();
     }
     store_operand<SPLIT, TR>(b_tile, breg, t);
-    if (j + 1 < nch) load_operand<SPLIT, TR>(breg, src, b_rows, C, (j + 1) * kAxKc, vec, t);
+    if (j + 1 < jhi) load_operand<SPLIT, TR>(breg, src, b_rows, C, (j + 1) * kAxKc, vec, t);
     cp_async_wait_all();
     ptx::fence_proxy_async_smem();
     ptx::tc_fence_before();
@@ -221,7 +229,7 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
         const uint32_t byte = (uint32_t)ks * 32u;
         const uint32_t offa = (byte >> 7) * kRegionBytes + (byte & 127u);
         const uint32_t offb = (byte >> 7) * Ge::kRegB + (byte & 127u);
-        const uint32_t acc = (j > 0 || ks > 0) ? 1u : 0u;
+        const uint32_t acc = (jj > 0 || ks > 0) ? 1u : 0u;
         const uint64_t ad = ptx::sw128_desc(a + offa), bd = ptx::sw128_desc(b + offb);
         if (SPLIT) {
           const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + offa);
@@ -237,8 +245,8 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
     }
   }
   if (ok) {  // the last commit covers every MMA issued before it
-    const int j = nch - 1;
-    const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[j & 1]), (uint32_t)((j >> 1) & 1), kWaitNs);
+    const int jj = jhi - 1 - jlo;
+    const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&bars[jj & 1]), (uint32_t)((jj >> 1) & 1), kWaitNs);
     ok = __syncthreads_and(w) != 0;
   }
   if (!ok) {
@@ -278,7 +286,7 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
 
 template <int TR>
 int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
-                   size_t img_stride, int* err, cudaStream_t s) {
+                   size_t img_stride, int reach, int* err, cudaStream_t s) {
   size_t done = 0;
   while (done < nimg) {
     size_t chunk = nimg - done;
@@ -287,10 +295,10 @@ int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, 
     const size_t smem = AxGeom<TR>::kSmem;
     if (ctx->precision == WDL_SPLIT_BF16)
       tc_axis_kernel<true, TR><<<grid, kAxThreads, smem, s>>>(in + done * img_stride, out + done * img_stride,
-                                                              G, R, C, img_stride, err);
+                                                              G, R, C, img_stride, reach, err);
     else
       tc_axis_kernel<false, TR><<<grid, kAxThreads, smem, s>>>(in + done * img_stride, out + done * img_stride,
-                                                               G, R, C, img_stride, err);
+                                                               G, R, C, img_stride, reach, err);
     WDL_LAUNCH_CHECK(ctx);
     done += chunk;
   }
@@ -298,9 +306,9 @@ int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, 
 }
 
 int tc_axis_dispatch(wdl_ctx* ctx, int TR, const float* in, float* out, const uint8_t* G, int R, int C,
-                     size_t nimg, size_t img_stride, int* err, cudaStream_t s) {
-  return TR == 64 ? tc_axis_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, err, s)
-                  : tc_axis_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, err, s);
+                     size_t nimg, size_t img_stride, int reach, int* err, cudaStream_t s) {
+  return TR == 64 ? tc_axis_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s)
+                  : tc_axis_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s);
 }
 
 // Default tile height: 64 while the 128-row grid would fill fewer than two
@@ -318,16 +326,16 @@ int tc_axis_default_height(const wdl_ctx* ctx, int R, int C, size_t nimg) {
 // MMAs for every output element (same K chunks, same order), so the choice
 // does not change results.
 int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
-                 size_t img_stride, int* err, cudaStream_t s) {
+                 size_t img_stride, int reach, int* err, cudaStream_t s) {
   const long long key[6] = {2, R, C, (long long)nimg, ctx->precision == WDL_SPLIT_BF16 ? 2 : 4, 0};
   for (const auto& e : ctx->tuned)
     if (!std::memcmp(e.key, key, sizeof(key)))
-      return tc_axis_dispatch(ctx, e.choice, in, out, G, R, C, nimg, img_stride, err, s);
+      return tc_axis_dispatch(ctx, e.choice, in, out, G, R, C, nimg, img_stride, reach, err, s);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
   const int dflt = tc_axis_default_height(ctx, R, C, nimg);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
-    return tc_axis_dispatch(ctx, dflt, in, out, G, R, C, nimg, img_stride, err, s);
+    return tc_axis_dispatch(ctx, dflt, in, out, G, R, C, nimg, img_stride, reach, err, s);
   const int cand[2] = {128, 64};
   int best = dflt;
   float best_ms = 1e30f;
@@ -336,9 +344,9 @@ int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, in
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
   int rc = WDL_OK;
   for (int c : cand) {
-    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, err, s))) break;
+    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, reach, err, s))) break;
     cudaEventRecord(e0, s);
-    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, err, s))) break;
+    if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, reach, err, s))) break;
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -398,12 +406,12 @@ int conv_stack_tc_axes(wdl_ctx* ctx, const float* in, float* out, float* tmp, si
   const size_t N = ctx->N;
   int rc;
   if (ctx->ndim == 2) {
-    if ((rc = tc_axis_pass(ctx, in, tmp, blocks[0], H, W, nimg, N, err, s))) return rc;
-    return tc_axis_pass(ctx, tmp, out, blocks[1], W, H, nimg, N, err, s);
+    if ((rc = tc_axis_pass(ctx, in, tmp, blocks[0], H, W, nimg, N, ctx->axis_reach[0], err, s))) return rc;
+    return tc_axis_pass(ctx, tmp, out, blocks[1], W, H, nimg, N, ctx->axis_reach[1], err, s);
   }
-  if ((rc = tc_axis_pass(ctx, in, out, blocks[0], D * H, W, nimg, N, err, s))) return rc;
-  if ((rc = tc_axis_pass(ctx, out, tmp, blocks[1], W * D, H, nimg, N, err, s))) return rc;
-  return tc_axis_pass(ctx, tmp, out, blocks[2], H * W, D, nimg, N, err, s);
+  if ((rc = tc_axis_pass(ctx, in, out, blocks[0], D * H, W, nimg, N, ctx->axis_reach[0], err, s))) return rc;
+  if ((rc = tc_axis_pass(ctx, out, tmp, blocks[1], W * D, H, nimg, N, ctx->axis_reach[1], err, s))) return rc;
+  return tc_axis_pass(ctx, tmp, out, blocks[2], H * W, D, nimg, N, ctx->axis_reach[2], err, s);
 }
 
 }  // namespace wdl

@@ -69,6 +69,9 @@ struct wdl_ctx {
   // Dense Gibbs factor of each axis, G[i][j] = max(EPSILON, exp(-(i-j)^2/gamma)),
   // stored row-major n x n in FP64 and FP32 (cpp/kernels.h:637-640).
   int axis_len[3] = {0, 0, 0};
+  // Largest |i - j| whose factor entry is non-zero in FP32, per axis: beyond it
+  // (exp(-d^2/gamma) under the FP32 range) the FP32 factor is exactly zero.
+  int axis_reach[3] = {0, 0, 0};
   double* G64[3] = {nullptr, nullptr, nullptr};
   float* G32[3] = {nullptr, nullptr, nullptr};
 
