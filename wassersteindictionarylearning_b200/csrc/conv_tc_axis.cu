@@ -23,6 +23,9 @@
 //
 // Precision as the 128-tile operator: kind::tf32, or split BF16 with
 // hi*hi + hi*lo + lo*hi accumulated in FP32 (kind::f16).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstring>
 
 #include "tc_common.cuh"
@@ -284,6 +287,249 @@ __global__ void __launch_bounds__(kAxThreads, TR == 64 ? 2 : 1)
   if (warp == 0) ptx::tmem_dealloc(d, TR);
 }
 
+// ---- copy-engine staged form ---------------------------------------------------------
+// The same output tile, K chunks (band-limited as above) and MMAs as
+// tc_axis_kernel, with both operands staged by the copy engine instead of the
+// CTA's loads: per K chunk, one tiled TMA load brings the FP32 image rows
+// r0..r0+TR-1, elements kb..kb+63 (zero outside the tensor), and one bulk copy
+// the ready-made factor block, into a ring of S stages that complete on one
+// transaction-count barrier each.  One thread keeps S-1 chunks in flight ahead
+// of the one being multiplied; the CTA's threads only convert the landed FP32
+// rows (SMEM -> BF16 hi/lo or TF32 operand, double-buffered) while the tensor
+// cores multiply the previous chunk.  The image is viewed as the 2-D tensor
+// [images * R][C] (row pitch C * 4 bytes, so C % 4 == 0 and a 16-byte aligned
+// base are required; other shapes take tc_axis_kernel).  The converted values,
+// the chunk order and the MMA sequence are tc_axis_kernel's, so both forms give
+// the same bits.  No multicast: every load reads this GPU's own memory for one
+// CTA.
+template <int TR>
+struct AxTmaGeom {
+  static constexpr int kStages = TR == 64 ? 3 : 2;
+  static constexpr uint32_t kRaw = TR * kAxKc * 4;  // FP32 rows of one chunk
+  static constexpr uint32_t kRegB = TR * 128;       // one 128-byte column block of the operand
+  static constexpr uint32_t kB = 2 * kRegB;         // converted operand (both planes / TF32 K 0-63)
+  static constexpr size_t kRaw0 = (size_t)kStages * kAxOperand;
+  static constexpr size_t kB0 = kRaw0 + (size_t)kStages * kRaw;
+  static constexpr size_t kBar0 = kB0 + 2 * (size_t)kB;
+  static constexpr size_t kSmem = kBar0 + 128 + 1024;
+};
+
+template <bool SPLIT, int TR>
+__global__ void __launch_bounds__(kAxThreads, 1)
+    tc_axis_tma_kernel(const __grid_constant__ CUtensorMap tmap, float* __restrict__ out,
+                       const uint8_t* __restrict__ gblocks, int R, int C, size_t img_stride, int reach, int* err) {
+  using Ge = AxTmaGeom<TR>;
+  constexpr int S = Ge::kStages;
+  using F = Fmt<SPLIT>;
+  constexpr int CE = SPLIT ? 8 : 4;
+  constexpr int CPR = kAxKc / CE;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + Ge::kBar0);  // [S] copies of a stage landed
+  uint64_t* mmab = full + S;                                       // [2] MMAs reading operand b done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mmab + 2);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int c0 = blockIdx.x * kAxTile, r0 = blockIdx.y * TR;
+  const int nch = (C + kAxKc - 1) / kAxKc;
+  const uint8_t* gsrc = gblocks + (size_t)blockIdx.x * nch * kAxOperand;
+  float* dst = out + (size_t)blockIdx.z * img_stride;
+  const int c_last = min(c0 + kAxTile, C) - 1;
+  const int jlo = max(0, c0 - reach) / kAxKc;
+  const int n = min(C - 1, c_last + reach) / kAxKc + 1 - jlo;
+  const int ybase = (int)blockIdx.z * R + r0;  // row of the 2-D view
+
+  if (t == 0) {
+    for (int q = 0; q < S; ++q) ptx::mbar_init(ptx::smem_addr(&full[q]), 1);
+    ptx::mbar_init(ptx::smem_addr(&mmab[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&mmab[1]), 1);
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tslot), TR);
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t d = *tslot;
+  const uint32_t id = ptx::idesc(F::fmt, 128, TR);
+
+  auto a_tile = [&](int q) { return base + (size_t)q * kAxOperand; };
+  auto raw_tile = [&](int q) { return base + Ge::kRaw0 + (size_t)q * Ge::kRaw; };
+  auto b_tile = [&](int b) { return base + Ge::kB0 + (size_t)b * Ge::kB; };
+  // thread 0: the copies of chunk jj into stage jj % S
+  auto issue = [&](int jj) {
+    const int q = jj % S;
+    const uint32_t bar = ptx::smem_addr(&full[q]);
+    ptx::mbar_arrive_expect_tx(bar, (uint32_t)kAxOperand + Ge::kRaw);
+    ptx::bulk_load(ptx::smem_addr(a_tile(q)), gsrc + (size_t)(jlo + jj) * kAxOperand, (uint32_t)kAxOperand, bar);
+    ptx::tma_load_2d(ptx::smem_addr(raw_tile(q)), &tmap, (jlo + jj) * kAxKc, ybase, bar);
+  };
+  int issued = 0;
+  if (t == 0)
+    for (; issued < S && issued < n; ++issued) issue(issued);
+
+  bool ok = true;
+  int jj = 0;
+  for (; jj < n; ++jj) {
+    const int q = jj % S, b = jj & 1;
+    // this chunk's copies have landed; the operand buffer b is no longer read
+    // by the MMAs of chunk jj - 2
+    bool w = ptx::mbar_wait(ptx::smem_addr(&full[q]), (uint32_t)((jj / S) & 1), kWaitNs);
+    if (jj >= 2) w = w && ptx::mbar_wait(ptx::smem_addr(&mmab[b]), (uint32_t)(((jj - 2) >> 1) & 1), kWaitNs);
+    ok = __syncthreads_and(w) != 0;
+    if (!ok) break;
+    {  // landed FP32 rows -> the operand (rows beyond the image are never stored)
+      const float* raw = reinterpret_cast<const float*>(raw_tile(q));
+      uint8_t* bt = b_tile(b);
+#pragma unroll
+      for (int u = 0; u < TR * CPR / kAxThreads; ++u) {
+        const int c = t + u * kAxThreads;
+        const int r = c / CPR, kk = (c - r * CPR) * CE;
+        float v[CE];
+#pragma unroll
+        for (int e = 0; e < CE; e += 4) {
+          const float4 f = *reinterpret_cast<const float4*>(raw + r * kAxKc + kk + e);
+          v[e] = f.x; v[e + 1] = f.y; v[e + 2] = f.z; v[e + 3] = f.w;
+        }
+        put_axis_chunk<SPLIT, Ge::kRegB>(bt, r, kk, v);
+      }
+    }
+    ptx::fence_proxy_async_smem();
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      ptx::tc_fence_after();
+      const uint32_t a = ptx::smem_addr(a_tile(q)), bb = ptx::smem_addr(b_tile(b));
+      const int steps = kAxKc / F::kstep;
+#pragma unroll
+      for (int ks = 0; ks < steps; ++ks) {
+        const uint32_t byte = (uint32_t)ks * 32u;
+        const uint32_t offa = (byte >> 7) * kRegionBytes + (byte & 127u);
+        const uint32_t offb = (byte >> 7) * Ge::kRegB + (byte & 127u);
+        const uint32_t acc = (jj > 0 || ks > 0) ? 1u : 0u;
+        const uint64_t ad = ptx::sw128_desc(a + offa), bd = ptx::sw128_desc(bb + offb);
+        if (SPLIT) {
+          const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + offa);
+          const uint64_t blo = ptx::sw128_desc(bb + Ge::kRegB + offb);
+          ptx::mma_bf16(d, ad, bd, id, acc);
+          ptx::mma_bf16(d, ad, blo, id, 1u);
+          ptx::mma_bf16(d, alo, bd, id, 1u);
+        } else {
+          ptx::mma_tf32(d, ad, bd, id, acc);
+        }
+      }
+      ptx::mma_commit(ptx::smem_addr(&mmab[b]));
+      // refill the stage of chunk jj - 1 once its MMAs are done (its factor
+      // block is read by them; its FP32 rows were converted last iteration)
+      if (jj >= 1 && issued < n) {
+        if (ptx::mbar_wait(ptx::smem_addr(&mmab[(jj - 1) & 1]), (uint32_t)(((jj - 1) >> 1) & 1), kWaitNs)) {
+          issue(issued);
+          ++issued;
+        } else {
+          atomicExch(err, WDL_ERR_TIMEOUT);
+        }
+      }
+    }
+  }
+  if (ok) {  // the last commit covers every MMA issued before it
+    const int last = n - 1;
+    const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&mmab[last & 1]), (uint32_t)((last >> 1) & 1), kWaitNs);
+    ok = __syncthreads_and(w) != 0;
+  }
+  if (!ok) {
+    if (t == 0) {
+      atomicExch(err, WDL_ERR_TIMEOUT);
+      // let the copies still in flight land (bounded) before the CTA's SMEM goes away
+      for (int p = jj; p < issued; ++p)
+        ptx::mbar_wait(ptx::smem_addr(&full[p % S]), (uint32_t)((p / S) & 1), kWaitNs);
+      if (jj >= 1)
+        ptx::mbar_wait(ptx::smem_addr(&mmab[(jj - 1) & 1]), (uint32_t)(((jj - 1) >> 1) & 1), kWaitNs);
+    }
+    __syncthreads();
+  } else {
+    ptx::tc_fence_after();
+    const int qd = warp & 3, half = warp >> 2;
+    const int c = c0 + qd * 32 + lane;
+    const bool rvec = (R & 3) == 0;
+#pragma unroll
+    for (int cc = 0; cc < TR / 32; ++cc) {
+      float v[16];
+      const int col = half * (TR / 2) + cc * 16;
+      ptx::tmem_ld16(d + ((uint32_t)(qd * 32) << 16) + (uint32_t)col, v);
+      ptx::tmem_ld_wait();
+      if (c < C) {
+        float* orow = dst + (size_t)c * R;
+        const int rb = r0 + col;
+#pragma unroll
+        for (int i = 0; i < 16; i += 4) {
+          const int r = rb + i;
+          if (rvec && r + 3 < R) {
+            *reinterpret_cast<float4*>(orow + r) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          } else {
+            for (int e = 0; e < 4; ++e)
+              if (r + e < R) orow[r + e] = v[i + e];
+          }
+        }
+      }
+    }
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  if (warp == 0) ptx::tmem_dealloc(d, TR);
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The copy-engine form applies: row pitch and base 16-byte aligned.
+bool tc_axis_tma_ok(const float* in, int C) {
+  return (C % 4) == 0 && (reinterpret_cast<uintptr_t>(in) % 16) == 0 && encode_tiled() != nullptr;
+}
+
+template <int TR>
+int tc_axis_tma_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
+                       size_t img_stride, int reach, int* err, cudaStream_t s) {
+  size_t done = 0;
+  while (done < nimg) {
+    size_t chunk = nimg - done;
+    if (chunk > 65535) chunk = 65535;
+    const float* src = in + done * img_stride;
+    // the chunk's images as the 2-D tensor [chunk * R][C] (image stride R * C)
+    CUtensorMap tmap;
+    const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)chunk * (cuuint64_t)R};
+    const cuuint64_t strides[1] = {(cuuint64_t)C * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kAxKc, (cuuint32_t)TR};
+    const cuuint32_t estr[2] = {1, 1};
+    if (img_stride != (size_t)R * C)
+      return set_error(ctx, WDL_ERR_UNSUPPORTED, "copy-engine axis pass: images must be contiguous");
+    const CUresult cr = encode_tiled()(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(src), dims,
+                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return set_error(ctx, WDL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    dim3 grid((C + kAxTile - 1) / kAxTile, (R + TR - 1) / TR, (unsigned)chunk);
+    const size_t smem = AxTmaGeom<TR>::kSmem;
+    if (ctx->precision == WDL_SPLIT_BF16)
+      tc_axis_tma_kernel<true, TR><<<grid, kAxThreads, smem, s>>>(tmap, out + done * img_stride, G, R, C,
+                                                                  img_stride, reach, err);
+    else
+      tc_axis_tma_kernel<false, TR><<<grid, kAxThreads, smem, s>>>(tmap, out + done * img_stride, G, R, C,
+                                                                   img_stride, reach, err);
+    WDL_LAUNCH_CHECK(ctx);
+    done += chunk;
+  }
+  return WDL_OK;
+}
+
 template <int TR>
 int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
                    size_t img_stride, int reach, int* err, cudaStream_t s) {
@@ -305,8 +551,15 @@ int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, 
   return WDL_OK;
 }
 
+// choice: the output tile height (64 or 128), plus 1000 for the copy-engine form
 int tc_axis_dispatch(wdl_ctx* ctx, int TR, const float* in, float* out, const uint8_t* G, int R, int C,
                      size_t nimg, size_t img_stride, int reach, int* err, cudaStream_t s) {
+  if (TR >= 1000) {
+    if (tc_axis_tma_ok(in, C))
+      return TR == 1064 ? tc_axis_tma_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s)
+                        : tc_axis_tma_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s);
+    TR -= 1000;  // an unaligned call of a tuned shape: the same tile from the CTA's loads
+  }
   return TR == 64 ? tc_axis_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s)
                   : tc_axis_launch<128>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s);
 }
@@ -336,14 +589,16 @@ int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, in
   const int dflt = tc_axis_default_height(ctx, R, C, nimg);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
     return tc_axis_dispatch(ctx, dflt, in, out, G, R, C, nimg, img_stride, reach, err, s);
-  const int cand[2] = {128, 64};
+  const int cand_all[4] = {128, 64, 1128, 1064};
+  const int ncand = tc_axis_tma_ok(in, C) && img_stride == (size_t)R * C ? 4 : 2;
   int best = dflt;
   float best_ms = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e0));
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
   int rc = WDL_OK;
-  for (int c : cand) {
+  for (int ci = 0; ci < ncand; ++ci) {
+    const int c = cand_all[ci];
     if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, reach, err, s))) break;
     cudaEventRecord(e0, s);
     if ((rc = tc_axis_dispatch(ctx, c, in, out, G, R, C, nimg, img_stride, reach, err, s))) break;
@@ -385,6 +640,14 @@ int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]) {
                                          (int)AxGeom<64>::kSmem));
   WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)AxGeom<64>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxTmaGeom<128>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxTmaGeom<128>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxTmaGeom<64>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)AxTmaGeom<64>::kSmem));
   const bool split = ctx->precision == WDL_SPLIT_BF16;
   for (int a = 0; a < ctx->ndim; ++a) {
     const int C = ctx->axis_len[a];
