@@ -73,7 +73,8 @@ def large():
     lam = init_weights(1, K, seed=73)[0]
     la, dic, bary = R.gradient_both_log(W, H, g, K, L, lt, atoms, lam, obs)
     out = dict(W=W, H=H, K=K, L=L, gamma=g, loss=lt, seeds=np.array([71, 72, 73]),
-               in_stats=in_stats(obs, atoms, lam), lambdas=lam, resultLa=la, bary=bary)
+               in_stats=in_stats(obs, atoms, lam), lambdas=lam, resultLa=la, bary=bary,
+               resultLa_scale=O.gradient_both_scale(W, H, 1, g, K, L, lt, atoms, lam, obs, log_domain=True))
     save_stats("gradlog_256x256_K8_L10_loss1", "resultDic", dic, out)
     save("full_gradlog_256x256_K8_L10_loss1", **out)
 

@@ -39,16 +39,28 @@ def _case(P=4, W=32, H=24, K=3, L=12, gamma=2.0, loss=2, seed=3):
     return cfg, obs, sol0
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 1e-5), ("split_bf16", 1e-3)])
-def test_device_regress_follows_host_lbfgs(precision, tol):
-    cfg, obs, sol0 = _case()
+# FP64 on a narrow kernel (gamma 2 px^2, scalings up to ~7e37 along the run);
+# the FP32 forms on a case whose scalings stay below ~4e10 over every trial
+# point of the run (a numpy FP64 replay of the forward recursion), so that
+# neither the host nor the device run meets the FP32 range limit.
+NARROW = dict(P=4, W=32, H=24, K=3, L=12, gamma=2.0, seed=3, iters=6)
+WIDE = dict(P=3, W=20, H=16, K=3, L=6, gamma=10.0, seed=5, iters=4)
+
+
+@pytest.mark.parametrize("precision,tol,case", [("fp64", 1e-9, NARROW), ("fp32", 1e-5, WIDE),
+                                                ("split_bf16", 1e-3, WIDE)])
+def test_device_regress_follows_host_lbfgs(precision, tol, case):
+    c = dict(case)
+    iters = c.pop("iters")
+    cfg, obs, sol0 = _case(**c)
     args = (cfg["W"], cfg["H"], cfg["gamma"], cfg["P"], cfg["K"], cfg["L"], 2, cfg["scale_dic"], obs, precision)
     host = _regression(*args)
-    host.wrTotalIteration = 6
+    host.wrTotalIteration = iters
     s_host = sol0.copy()
     st_host = host.regress_both(s_host)
+    assert np.isfinite(s_host).all()
     dev = _regression(*args)
-    dev.wrTotalIteration = 6
+    dev.wrTotalIteration = iters
     s_dev = sol0.copy()
     st_dev = dev.regress_both_device(s_dev)
     assert st_dev == st_host

@@ -84,23 +84,17 @@ __device__ __forceinline__ double st_sum(double v, double* scratch, int st, int 
   return tot;
 }
 
-// Pulls an image's 128-byte lines into L2 ahead of use (no registers, no wait).
-#ifndef WDL_X_BULKPF
-#define WDL_X_BULKPF 0
-#endif
+// Pulls an image into L2 ahead of use with one bulk prefetch by the copy
+// engine (its 16-byte aligned interior), issued by one thread: no registers,
+// no wait, and no load-unit traffic in the issuing stream (thread-issued
+// per-line prefetches cost the reverse items ~1.4 us of issue each).
 __device__ __forceinline__ void prefetch_l2(const float* p, size_t n, int t) {
-#if WDL_X_BULKPF
-  // one bulk prefetch by the copy engine: the 16-byte aligned interior of the image
   if (t == 0) {
     const uintptr_t a0 = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
     const uintptr_t a1 = (reinterpret_cast<uintptr_t>(p + n)) & ~uintptr_t(15);
     if (a1 > a0)
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((uint32_t)(a1 - a0)) : "memory");
   }
-#else
-  for (size_t off = (size_t)t * 32; off < n; off += (size_t)kSt * 32)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
-#endif
 }
 
 // L2 eviction priority of a global access: normal, evict-first (the last use
@@ -207,11 +201,7 @@ template <bool SPLIT, int NIN, uint32_t HS = 0, class F>
 __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
                                            F f, const Geo& g, int t) {
   constexpr int CE = SPLIT ? 8 : 4;
-#ifndef WDL_X_UNR
   constexpr int UNR = NIN > 2 ? 1 : 2;
-#else
-  constexpr int UNR = NIN > 2 ? WDL_X_UNR : 2;
-#endif
   const int total = g.Hp * (int)g.cpr;
   for (int base = t; base < total; base += kSt * UNR) {
     float in[UNR][NIN > 0 ? NIN : 1][CE];
@@ -391,11 +381,7 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
   bar_sync(c.st, kSt);
   const int j = c.t & 31;  // 16-byte chunk of the row
   const int x0 = 4 * j;
-#ifndef WDL_X_U
   constexpr int U = 2;
-#else
-  constexpr int U = WDL_X_U;
-#endif
   for (int i0 = c.t >> 5; i0 < g.H; i0 += kWarps * U) {
     float4 y4[U];
     float in[U][NIN > 0 ? NIN : 1][4];
