@@ -245,8 +245,16 @@ struct Ctl {
 // lane; warps w and w+4 of the stream take alternate 16-column chunks of the
 // same lanes) -> MMA2 (A from tensor memory, B = G) -> D2 in D1's columns.
 // Column form: K1 = Wp, N1 = Hp; row form: K1 = Hp, N1 = Wp.
+template <bool SPLIT, class PRE>
+__device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre);
 template <bool SPLIT>
 __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
+  return gemm_pair<SPLIT>(c, K1, N1, [] {});
+}
+// The same, running pre() (loads that do not depend on the result) while the
+// first GEMM runs.
+template <bool SPLIT, class PRE>
+__device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre) {
   ptx::tc_fence_before();
   ptx::fence_proxy_async_smem();
   bar_sync(c.st, kSt);
@@ -255,6 +263,7 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
     issue_gemm<SPLIT>(c.d1, c.g_a, c.x_a, K1, N1);
     ptx::mma_commit(c.bar_a);
   }
+  pre();
   bool ok = bar_all(ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
   c.phase ^= 1;
   ptx::tc_fence_after();
@@ -301,11 +310,18 @@ __device__ __forceinline__ void load_col_chunk(float (&in)[NIN][16], const float
 
 template <bool SPLIT, int NIN, uint32_t HS = 0, class M>
 __device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
-                                            bool stage_next) {
+                                            bool stage_next, const float (*first)[16] = nullptr) {
   const int x = c.lane_row;
   for (int c0 = 16 * c.half; c0 < g.Hp; c0 += 32) {
     float in[NIN][16];
-    load_col_chunk<NIN, HS, 0>(in, src, c0, x, g);
+    if (first && c0 == 16 * c.half) {  // this thread's first chunk, loaded during the GEMMs
+#pragma unroll
+      for (int q = 0; q < NIN; ++q)
+#pragma unroll
+        for (int t = 0; t < 16; ++t) in[q][t] = first[q][t];
+    } else {
+      load_col_chunk<NIN, HS, 0>(in, src, c0, x, g);
+    }
     float y[16];
     ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
     ptx::tmem_ld_wait();
@@ -482,6 +498,9 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
 #ifndef WDL_X_EARLY
 #define WDL_X_EARLY 0
 #endif
+#ifndef WDL_X_PREMID
+#define WDL_X_PREMID 0
+#endif
   int next_item = -1;  // thread 0: the item claimed during the previous completion
   while (true) {
     tr.start(a.trace, t);
@@ -621,14 +640,20 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         stage_rows<SPLIT, 2>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
       }
       tr.mark(2);
+      const float* msrc[1] = {atom};
+#if WDL_X_PREMID
+      float pin[1][16];
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp, [&] { load_col_chunk<1, hints(kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
+#else
+      const float (*pin)[16] = nullptr;
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+#endif
       tr.mark(3);
       const bool keep_cb = !fwd_only;
-      const float* msrc[1] = {atom};
       mid_columns<SPLIT, 1, hints(kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
         if (keep_cb) stg1<kHF>(cb_out + idx, y);  // read again only in the reverse pass
         return fdiv(in[0], y);
-      }, true);
+      }, true, pin);
       tr.mark(4);
       ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
       tr.mark(5);
@@ -650,17 +675,24 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
           c.tile, src, [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); }, g,
           t);
       tr.mark(2);
-      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
-      tr.mark(3);
       const float* cbp = pr->cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
       float* gd = pr->gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
+#if WDL_X_PREMID
+      float pin[3][16];
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp,
+                            [&] { load_col_chunk<3, hints(kHF, kHL, kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
+#else
+      const float (*pin)[16] = nullptr;
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+#endif
+      tr.mark(3);
       mid_columns<SPLIT, 3, hints(kHF, kHL, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
         const float rc = frcp(in[0]);
         const float q2 = y * rc;
         stg1<kHL>(gd + idx, in[1] + q2);
         return -in[2] * q2 * rc;
-      }, s > 1);
+      }, s > 1, pin);
       tr.mark(4);
       if (s > 1) {
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
@@ -690,14 +722,21 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       if (t == 0) atomicAdd(&pr->dot[pk], dsum);
       tr.mark(2);
       if (s > 1) {
-        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
-        tr.mark(3);
         const float* cbp = pr->cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
+#if WDL_X_PREMID
+        float pin[2][16];
+        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp,
+                              [&] { load_col_chunk<2, hints(kHF, kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
+#else
+        const float (*pin)[16] = nullptr;
+        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
+#endif
+        tr.mark(3);
         mid_columns<SPLIT, 2, hints(kHF, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
           return y * (-in[1] * rc * rc);
-        }, true);
+        }, true, pin);
         tr.mark(4);
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
         tr.mark(5);
