@@ -378,7 +378,8 @@ __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x)
 #endif
 template <int NIN, uint32_t HS = 0, int RH = kHN, class E>
 __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
-                                             float* acc, E e, int rot = 0) {
+                                             float* acc, E e, int rot = 0,
+                                             const float (*first)[NIN > 0 ? NIN : 1][4] = nullptr) {
   {
     const int i = c.lane_row;
     uint8_t* rowp = c.tile + (size_t)i * 512;
@@ -416,7 +417,14 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
       y4[u] = okr ? *reinterpret_cast<const float4*>(c.tile + (size_t)i * 512 + ((j ^ (i & 7)) << 4))
                   : make_float4(0.f, 0.f, 0.f, 0.f);
       const size_t idx = (size_t)i * g.W + x0;
-      load_px4<NIN, HS, 0>(in[u], src, idx, okr, x0, g);
+      if (first && i0 == (c.t >> 5)) {  // loaded during the GEMMs
+#pragma unroll
+        for (int q = 0; q < (NIN > 0 ? NIN : 1); ++q)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) in[u][q][r] = first[u][q][r];
+      } else {
+        load_px4<NIN, HS, 0>(in[u], src, idx, okr, x0, g);
+      }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -432,6 +440,20 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
         for (int r = 0; r < nv; ++r) atomicAdd(acc + idx + r, o[r]);
       }
     }
+  }
+}
+
+// The inputs of the epilogue's first two rows for this thread (rows t/32 and
+// t/32 + 8, pixels 4 (t % 32) ..), for loading while the GEMMs run.
+template <int NIN, uint32_t HS>
+__device__ __forceinline__ void epi_first_loads(float (&pre)[2][NIN][4], const Ctl& c, const Geo& g,
+                                                const float* const (&src)[NIN]) {
+  const int x0 = 4 * (c.t & 31);
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int i = (c.t >> 5) + u * kWarps;
+    const bool okr = i < g.H && x0 < g.W;
+    load_px4<NIN, HS, 0>(pre[u], src, (size_t)i * g.W + x0, okr, x0, g);
   }
 }
 
@@ -500,6 +522,9 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
 #endif
 #ifndef WDL_X_PREMID
 #define WDL_X_PREMID 0
+#endif
+#ifndef WDL_X_PREEPI
+#define WDL_X_PREEPI 0
 #endif
   int next_item = -1;  // thread 0: the item claimed during the previous completion
   while (true) {
@@ -695,18 +720,24 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       }, s > 1, pin);
       tr.mark(4);
       if (s > 1) {
-        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
-        tr.mark(5);
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
+        const float* esrc[1] = {php};
+#if WDL_X_PREEPI && !WDL_X_ROT
+        float epre[2][1][4];
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp, [&] { epi_first_loads<1, hints(kHN)>(epre, c, g, esrc); });
+#else
+        const float (*epre)[1][4] = nullptr;
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+#endif
+        tr.mark(5);
         float* vout = pr->v + pk * N;
         float* nout = pr->nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        const float* esrc[1] = {php};
         epi_rows_red<1, hints(kHN), kHL>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
           const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
                                         fdiv(y.w, in[0][3]));
           st4<kHL>(vout + idx, vv, nv, g.vec);
           return vv;
-        }, rot);
+        }, rot, epre);
         tr.mark(6);
       }
     } else {  // ---------------- reverse pass, weight recursion
@@ -738,13 +769,19 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
           return y * (-in[1] * rc * rc);
         }, true, pin);
         tr.mark(4);
-        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
-        tr.mark(5);
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
         const float* accp = pr->acc + slot(s - 1) * PN + (size_t)p * N;
+        const float* esrc[2] = {accp, php};
+#if WDL_X_PREEPI && !WDL_X_ROT
+        float epre[2][2][4];
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp, [&] { epi_first_loads<2, hints(kHN, kHN)>(epre, c, g, esrc); });
+#else
+        const float (*epre)[2][4] = nullptr;
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
+#endif
+        tr.mark(5);
         float* rout = pr->r + pk * N;
         float* gout = pr->gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        const float* esrc[2] = {accp, php};
         epi_rows_red<2, hints(kHN, kHN), kHL>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
           const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
                                         y.y * fdiv(__expf(in[0][1]), in[1][1]),
@@ -752,7 +789,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
                                         y.w * fdiv(__expf(in[0][3]), in[1][3]));
           st4<kHL>(rout + idx, rr, nv, g.vec);
           return rr;
-        }, rot);
+        }, rot, epre);
         tr.mark(6);
       }
     }
