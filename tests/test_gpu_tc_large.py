@@ -71,7 +71,8 @@ def test_axis_tile_heights_agree(shape, precision):
     """The axis pass has two tile heights (128 image rows, one CTA per SM; 64
     rows, two CTAs per SM) and two ways of staging its operands (the CTA's own
     loads, or TMA / bulk copies on a stage ring where the row pitch allows),
-    chosen per shape by timing every variant on the call's own data.  All issue
+    and a persistent form that keeps the factor slab resident in SMEM, chosen per
+    shape by timing every variant on the call's own data.  All issue
     the same MMAs on the same operand values for every output element (same K
     chunks in the same order), so the tuned context returns exactly what a
     context held at the default returns; the tuning call's result is the last
@@ -95,8 +96,9 @@ def test_axis_tile_heights_agree(shape, precision):
     for i in range(n):
         check(lib().wdl_autotune_entry(tuned.ctx, i, key, C.byref(choice), C.byref(ms)), tuned.ctx)
         if key[0] == 2:
-            # tile height 64 or 128, plus 1000 for the copy-engine (TMA) staged form
-            assert choice.value in (64, 128, 1064, 1128) and ms.value > 0
+            # tile height 64 or 128, plus 1000 for the copy-engine (TMA) staged form;
+            # 2064 the persistent form with the factor slab resident in SMEM
+            assert choice.value in (64, 128, 1064, 1128, 2064) and ms.value > 0
             heights.append(choice.value)
     assert len(heights) == (2 if D == 1 else 3)  # one entry per axis-pass shape
     assert lib().wdl_autotune_count(plain.ctx) == 0

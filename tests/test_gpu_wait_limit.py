@@ -47,11 +47,13 @@ def test_dependency_wait_runs_out_and_context_recovers():
     assert err.value.code == WDL_ERR_TIMEOUT, str(err.value)
     assert elapsed < 2.0, elapsed
 
-    # the context is still usable: default bound, no fault, same results as a fresh context
+    # the context is still usable: default bound, no fault, the results of a fresh
+    # context (the fused kernel's float atomics make repeated runs agree to the
+    # split-BF16 rounding, not bitwise: barycenter and loss 1e-4, gradients 1e-3)
     assert L.wdl_set_wait_limit(k.ctx, 0.0) == 0
     out = batch_run(k, probs)
-    for key in ("la", "loss", "bary", "dic"):
-        assert rel(out[0][key], ref[0][key]) < 1e-5, key
+    for key, tol in (("bary", 1e-4), ("loss", 1e-4), ("la", 1e-3), ("dic", 1e-3)):
+        assert rel(out[0][key], ref[0][key]) < tol, key
 
 
 def test_wait_limit_arguments():

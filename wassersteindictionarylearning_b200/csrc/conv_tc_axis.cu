@@ -477,6 +477,220 @@ __global__ void __launch_bounds__(kAxThreads, 1)
   if (warp == 0) ptx::tmem_dealloc(d, TR);
 }
 
+// ---- persistent, factor-resident form ------------------------------------------------
+// A CTA owns one 128-row slab c0.. of the factor and keeps its band-limited K
+// chunks resident in SMEM (loaded once by bulk copies), then walks a strided
+// share of the (image, 64-row tile) pairs: per tile and chunk one TMA load of
+// the FP32 image rows (two stages), the conversion into the operand (two
+// buffers) and the MMAs into one of two TMEM accumulators, so that a tile's
+// epilogue (TMEM -> its output rows) runs while the tensor cores work on the
+// next tile.  The per-tile factor reloads of the tiled forms (4 of every 6 bytes
+// they move) disappear.  Same operand values, chunk order and MMAs per output
+// tile as the other forms, so the same bits.
+constexpr int kPxTR = 64;         // image rows per tile (MMA N)
+constexpr int kPxMaxChunks = 5;   // resident factor chunks (5 x 32 KB)
+struct PxGeom {
+  static constexpr uint32_t kRaw = kPxTR * kAxKc * 4;   // 16 KB
+  static constexpr uint32_t kRegB = kPxTR * 128;
+  static constexpr uint32_t kB = 2 * kRegB;             // 16 KB
+  static constexpr size_t kRaw0 = (size_t)kPxMaxChunks * kAxOperand;
+  static constexpr size_t kB0 = kRaw0 + 2 * (size_t)kRaw;
+  static constexpr size_t kBar0 = kB0 + 2 * (size_t)kB;
+  static constexpr size_t kSmem = kBar0 + 128 + 1024;
+};
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(kAxThreads, 1)
+    tc_axis_persist_kernel(const __grid_constant__ CUtensorMap tmap, float* __restrict__ out,
+                           const uint8_t* __restrict__ gblocks, int R, int C, int nimg, size_t img_stride,
+                           int reach, int* err) {
+  using Ge = PxGeom;
+  using F = Fmt<SPLIT>;
+  constexpr int CE = SPLIT ? 8 : 4;
+  constexpr int CPR = kAxKc / CE;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + Ge::kBar0);  // [2] image chunk landed
+  uint64_t* mmab = full + 2;                                       // [2] MMAs reading operand b done
+  uint64_t* fbar = mmab + 2;                                       // factor slab landed
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fbar + 1);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int c0 = blockIdx.x * kAxTile;
+  const int nch = (C + kAxKc - 1) / kAxKc;
+  const int c_last = min(c0 + kAxTile, C) - 1;
+  const int jlo = max(0, c0 - reach) / kAxKc;
+  const int nk = min(C - 1, c_last + reach) / kAxKc + 1 - jlo;  // <= kPxMaxChunks (host-checked)
+  const int rtiles = (R + kPxTR - 1) / kPxTR;
+  const int ntile_all = nimg * rtiles;
+  // this CTA's tiles: blockIdx.y, blockIdx.y + gridDim.y, ...
+  const int my_tiles = blockIdx.y < ntile_all ? (ntile_all - 1 - (int)blockIdx.y) / (int)gridDim.y + 1 : 0;
+  const int nsteps = my_tiles * nk;
+
+  if (t == 0) {
+    ptx::mbar_init(ptx::smem_addr(&full[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&full[1]), 1);
+    ptx::mbar_init(ptx::smem_addr(&mmab[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&mmab[1]), 1);
+    ptx::mbar_init(ptx::smem_addr(fbar), 1);
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tslot), 2 * kPxTR);
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t d0 = *tslot;
+  const uint32_t id = ptx::idesc(F::fmt, 128, kPxTR);
+
+  auto raw_tile = [&](int q) { return base + Ge::kRaw0 + (size_t)q * Ge::kRaw; };
+  auto b_tile = [&](int b) { return base + Ge::kB0 + (size_t)b * Ge::kB; };
+  // step g = (tile i, chunk jj): its image chunk into raw stage g & 1
+  auto issue = [&](int g) {
+    const int i = g / nk, jj = g - i * nk;
+    const int tile = (int)blockIdx.y + i * (int)gridDim.y;
+    const int z = tile / rtiles, r0 = (tile - z * rtiles) * kPxTR;
+    const uint32_t bar = ptx::smem_addr(&full[g & 1]);
+    ptx::mbar_arrive_expect_tx(bar, Ge::kRaw);
+    ptx::tma_load_2d(ptx::smem_addr(raw_tile(g & 1)), &tmap, (jlo + jj) * kAxKc, z * R + r0, bar);
+  };
+  int issued = 0, committed = 0;  // thread 0: image chunks requested, steps whose MMAs are issued
+  if (t == 0 && nsteps > 0) {
+    const uint32_t fb = ptx::smem_addr(fbar);
+    ptx::mbar_arrive_expect_tx(fb, (uint32_t)(nk * kAxOperand));
+    const uint8_t* gsrc = gblocks + ((size_t)blockIdx.x * nch + jlo) * kAxOperand;
+    for (int jj = 0; jj < nk; ++jj)
+      ptx::bulk_load(ptx::smem_addr(base + (size_t)jj * kAxOperand), gsrc + (size_t)jj * kAxOperand,
+                     (uint32_t)kAxOperand, fb);
+    for (; issued < 2 && issued < nsteps; ++issued) issue(issued);
+  }
+  bool ok = nsteps == 0 || __syncthreads_and(t != 0 || ptx::mbar_wait(ptx::smem_addr(fbar), 0, kWaitNs)) != 0;
+
+  // epilogue of tile i (accumulator i & 1): TMEM -> out[c][r0 ..]
+  auto epilogue = [&](int i) {
+    const int tile = (int)blockIdx.y + i * (int)gridDim.y;
+    const int z = tile / rtiles, r0 = (tile - z * rtiles) * kPxTR;
+    float* dst = out + (size_t)z * img_stride;
+    const uint32_t d = d0 + (uint32_t)((i & 1) * kPxTR);
+    const int qd = warp & 3, half = warp >> 2;
+    const int c = c0 + qd * 32 + lane;
+    const bool rvec = (R & 3) == 0;
+#pragma unroll
+    for (int cc = 0; cc < kPxTR / 32; ++cc) {
+      float v[16];
+      const int col = half * (kPxTR / 2) + cc * 16;
+      ptx::tmem_ld16(d + ((uint32_t)(qd * 32) << 16) + (uint32_t)col, v);
+      ptx::tmem_ld_wait();
+      if (c < C) {
+        float* orow = dst + (size_t)c * R;
+        const int rb = r0 + col;
+#pragma unroll
+        for (int e = 0; e < 16; e += 4) {
+          const int r = rb + e;
+          if (rvec && r + 3 < R) {
+            *reinterpret_cast<float4*>(orow + r) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+          } else {
+            for (int q = 0; q < 4; ++q)
+              if (r + q < R) orow[r + q] = v[e + q];
+          }
+        }
+      }
+    }
+  };
+
+  int g = 0;
+  for (; ok && g < nsteps; ++g) {
+    const int i = g / nk, jj = g - i * nk, b = g & 1;
+    bool w = ptx::mbar_wait(ptx::smem_addr(&full[g & 1]), (uint32_t)((g >> 1) & 1), kWaitNs);
+    if (g >= 2) w = w && ptx::mbar_wait(ptx::smem_addr(&mmab[b]), (uint32_t)(((g - 2) >> 1) & 1), kWaitNs);
+    ok = __syncthreads_and(w) != 0;
+    if (!ok) break;
+    {  // landed FP32 rows -> the operand
+      const float* raw = reinterpret_cast<const float*>(raw_tile(g & 1));
+      uint8_t* bt = b_tile(b);
+#pragma unroll
+      for (int u = 0; u < kPxTR * CPR / kAxThreads; ++u) {
+        const int cidx = t + u * kAxThreads;
+        const int r = cidx / CPR, kk = (cidx - r * CPR) * CE;
+        float v[CE];
+#pragma unroll
+        for (int e = 0; e < CE; e += 4) {
+          const float4 f4 = *reinterpret_cast<const float4*>(raw + r * kAxKc + kk + e);
+          v[e] = f4.x; v[e + 1] = f4.y; v[e + 2] = f4.z; v[e + 3] = f4.w;
+        }
+        put_axis_chunk<SPLIT, Ge::kRegB>(bt, r, kk, v);
+      }
+    }
+    ptx::fence_proxy_async_smem();
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      ptx::tc_fence_after();
+      // the raw stage is converted: refill it with step g + 2
+      if (issued < nsteps) {
+        issue(issued);
+        ++issued;
+      }
+      const uint32_t a = ptx::smem_addr(base + (size_t)jj * kAxOperand), bb = ptx::smem_addr(b_tile(b));
+      const uint32_t d = d0 + (uint32_t)((i & 1) * kPxTR);
+      const int steps = kAxKc / F::kstep;
+#pragma unroll
+      for (int ks = 0; ks < steps; ++ks) {
+        const uint32_t byte = (uint32_t)ks * 32u;
+        const uint32_t offa = (byte >> 7) * kRegionBytes + (byte & 127u);
+        const uint32_t offb = (byte >> 7) * Ge::kRegB + (byte & 127u);
+        const uint32_t acc = (jj > 0 || ks > 0) ? 1u : 0u;
+        const uint64_t ad = ptx::sw128_desc(a + offa), bd = ptx::sw128_desc(bb + offb);
+        if (SPLIT) {
+          const uint64_t alo = ptx::sw128_desc(a + kRegionBytes + offa);
+          const uint64_t blo = ptx::sw128_desc(bb + Ge::kRegB + offb);
+          ptx::mma_bf16(d, ad, bd, id, acc);
+          ptx::mma_bf16(d, ad, blo, id, 1u);
+          ptx::mma_bf16(d, alo, bd, id, 1u);
+        } else {
+          ptx::mma_tf32(d, ad, bd, id, acc);
+        }
+      }
+      ptx::mma_commit(ptx::smem_addr(&mmab[b]));
+      ++committed;
+    }
+    // the previous tile's accumulator is complete once the MMAs of its last
+    // chunk (step g - 1) are: store it while this tile's chunks multiply
+    if (jj == 0 && i > 0) {
+      const bool we = t != 0 || ptx::mbar_wait(ptx::smem_addr(&mmab[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1), kWaitNs);
+      ok = __syncthreads_and(we) != 0;
+      if (!ok) break;
+      ptx::tc_fence_after();
+      epilogue(i - 1);
+      // the next MMAs into this accumulator (tile i + 1) come after this sync
+      ptx::tc_fence_before();
+      __syncthreads();
+    }
+  }
+  if (ok && nsteps > 0) {  // the last tile
+    const int last = nsteps - 1;
+    const bool w = t != 0 || ptx::mbar_wait(ptx::smem_addr(&mmab[last & 1]), (uint32_t)((last >> 1) & 1), kWaitNs);
+    ok = __syncthreads_and(w) != 0;
+    if (ok) {
+      ptx::tc_fence_after();
+      epilogue(my_tiles - 1);
+    }
+  }
+  if (!ok) {
+    if (t == 0) {
+      atomicExch(err, WDL_ERR_TIMEOUT);
+      // let copies and MMAs still in flight finish (bounded) before the SMEM and TMEM go away
+      ptx::mbar_wait(ptx::smem_addr(fbar), 0, kWaitNs);
+      for (int q = g; q < issued; ++q) ptx::mbar_wait(ptx::smem_addr(&full[q & 1]), (uint32_t)((q >> 1) & 1), kWaitNs);
+      if (committed >= 1)
+        ptx::mbar_wait(ptx::smem_addr(&mmab[(committed - 1) & 1]), (uint32_t)(((committed - 1) >> 1) & 1), kWaitNs);
+    }
+    __syncthreads();
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  if (warp == 0) ptx::tmem_dealloc(d0, 2 * kPxTR);
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime.
 PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -530,6 +744,57 @@ int tc_axis_tma_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t*
   return WDL_OK;
 }
 
+// The factor-resident form applies when every slab's band-limited chunks fit
+// the resident buffer (and the copy-engine form applies).
+bool tc_axis_persist_ok(const float* in, int C, int reach) {
+  if (!tc_axis_tma_ok(in, C)) return false;
+  for (int c0 = 0; c0 < C; c0 += kAxTile) {
+    const int c_last = (c0 + kAxTile < C ? c0 + kAxTile : C) - 1;
+    const int lo = (c0 - reach > 0 ? c0 - reach : 0) / kAxKc;
+    const int hi = (c_last + reach < C - 1 ? c_last + reach : C - 1) / kAxKc + 1;
+    if (hi - lo > kPxMaxChunks) return false;
+  }
+  return true;
+}
+
+int tc_axis_persist_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C,
+                           size_t nimg, size_t img_stride, int reach, int* err, cudaStream_t s) {
+  if (img_stride != (size_t)R * C)
+    return set_error(ctx, WDL_ERR_UNSUPPORTED, "factor-resident axis pass: images must be contiguous");
+  const size_t max_imgs = ((size_t)1 << 30) / ((size_t)R + 1);  // keep tile indices in int
+  size_t done = 0;
+  while (done < nimg) {
+    size_t chunk = nimg - done;
+    if (chunk > max_imgs) chunk = max_imgs;
+    const float* src = in + done * img_stride;
+    CUtensorMap tmap;
+    const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)chunk * (cuuint64_t)R};
+    const cuuint64_t strides[1] = {(cuuint64_t)C * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kAxKc, (cuuint32_t)kPxTR};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult cr = encode_tiled()(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(src), dims,
+                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return set_error(ctx, WDL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    const int nslab = (C + kAxTile - 1) / kAxTile;
+    const long long tiles = (long long)chunk * ((R + kPxTR - 1) / kPxTR);
+    long long per = ctx->sm_count / nslab;
+    if (per < 1) per = 1;
+    if (per > tiles) per = tiles;
+    dim3 grid((unsigned)nslab, (unsigned)per);
+    if (ctx->precision == WDL_SPLIT_BF16)
+      tc_axis_persist_kernel<true><<<grid, kAxThreads, PxGeom::kSmem, s>>>(tmap, out + done * img_stride, G, R, C,
+                                                                          (int)chunk, img_stride, reach, err);
+    else
+      tc_axis_persist_kernel<false><<<grid, kAxThreads, PxGeom::kSmem, s>>>(tmap, out + done * img_stride, G, R, C,
+                                                                           (int)chunk, img_stride, reach, err);
+    WDL_LAUNCH_CHECK(ctx);
+    done += chunk;
+  }
+  return WDL_OK;
+}
+
 template <int TR>
 int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, int R, int C, size_t nimg,
                    size_t img_stride, int reach, int* err, cudaStream_t s) {
@@ -551,9 +816,15 @@ int tc_axis_launch(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, 
   return WDL_OK;
 }
 
-// choice: the output tile height (64 or 128), plus 1000 for the copy-engine form
+// choice: the output tile height (64 or 128), plus 1000 for the copy-engine
+// form; 2064 the persistent factor-resident form
 int tc_axis_dispatch(wdl_ctx* ctx, int TR, const float* in, float* out, const uint8_t* G, int R, int C,
                      size_t nimg, size_t img_stride, int reach, int* err, cudaStream_t s) {
+  if (TR == 2064) {
+    if (tc_axis_persist_ok(in, C, reach) && img_stride == (size_t)R * C)
+      return tc_axis_persist_launch(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s);
+    TR = 64;  // an unaligned call of a tuned shape: the same tile from the CTA's loads
+  }
   if (TR >= 1000) {
     if (tc_axis_tma_ok(in, C))
       return TR == 1064 ? tc_axis_tma_launch<64>(ctx, in, out, G, R, C, nimg, img_stride, reach, err, s)
@@ -589,8 +860,13 @@ int tc_axis_pass(wdl_ctx* ctx, const float* in, float* out, const uint8_t* G, in
   const int dflt = tc_axis_default_height(ctx, R, C, nimg);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
     return tc_axis_dispatch(ctx, dflt, in, out, G, R, C, nimg, img_stride, reach, err, s);
-  const int cand_all[4] = {128, 64, 1128, 1064};
-  const int ncand = tc_axis_tma_ok(in, C) && img_stride == (size_t)R * C ? 4 : 2;
+  int cand_all[5] = {128, 64, 0, 0, 0};
+  int ncand = 2;
+  if (tc_axis_tma_ok(in, C) && img_stride == (size_t)R * C) {
+    cand_all[ncand++] = 1128;
+    cand_all[ncand++] = 1064;
+    if (tc_axis_persist_ok(in, C, reach)) cand_all[ncand++] = 2064;
+  }
   int best = dflt;
   float best_ms = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -640,6 +916,10 @@ int tc_axis_init(wdl_ctx* ctx, uint8_t* (&blocks)[3]) {
                                          (int)AxGeom<64>::kSmem));
   WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)AxGeom<64>::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_persist_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)PxGeom::kSmem));
+  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_persist_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)PxGeom::kSmem));
   WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)AxTmaGeom<128>::kSmem));
   WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(tc_axis_tma_kernel<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
