@@ -448,7 +448,7 @@ def run_ours(args):
     # The other precisions on the same inputs, timed the same way (CUDA events on
     # the same stream, max over ranks): plain FP32 on the CUDA cores is the
     # metric's "vs plain FP32"; FP64 on the GPU is the reference's arithmetic.
-    arms, report = None, None
+    arms, report, regress_fp64 = None, None, None
     if wl["name"] == "batched128" and wl["domain"] == "kernel" and not args.no_arms:
         outs = {precision: run_outputs(L_, ctx, wl, x_d, obs_d, sd, sptr, dev)}
         arms = {}
@@ -458,6 +458,10 @@ def run_ours(args):
             k2 = w.CudaGaussian2DKernel(wl["gamma"], W, H, precision=prec, device=local)
             arms[prec] = time_arm(L_, k2.ctx, wl, x_d, obs_d, sd, sptr, dev, args, world, dist)
             outs[prec] = run_outputs(L_, k2.ctx, wl, x_d, obs_d, sd, sptr, dev)
+            if prec == "fp64" and not args.no_regress and world == 1:
+                # dictionary learning wholly on the device in the reference's arithmetic
+                regress_fp64 = time_regress(L_, k2.ctx, wl, wts, atoms, obs_d, sd, sptr, dev,
+                                            iters=args.regress_iters)
             k2.close()
             torch.cuda.synchronize()
         if "fp64" in outs and rank == 0:
@@ -498,7 +502,9 @@ def run_ours(args):
                             autotuned=tuned or None,
                             objective=fval),
                 roofline=roofline, cpu_baseline=cpu, e2e=e2e, gpu_launches=int(gpu_launches),
-                clocks=clocks, serving=serving, regress_both_device=regress)
+                clocks=clocks, serving=serving,
+                regress_both_device=dict(headline_precision=regress, fp64=regress_fp64)
+                if (regress or regress_fp64) else None)
     if arms:
         for prec, a in arms.items():
             line[f"value_{prec}"] = a["value"]
@@ -532,6 +538,9 @@ def time_regress(L_, ctx, wl, wts, atoms, obs_d, sd, sptr, dev, iters=3):
     ev1.record()
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
+    # status -1021 (LBFGSERR_CANCELED): a line-search trial's objective was NaN and
+    # the run stopped there, as the reference's progress_both stops it; on the FP32
+    # forms that is a trial point whose scalings leave the float range
     return dict(iterations=iters, evaluations=evals.value, status=status.value, objective=fval.value,
                 ms=ms, lbfgs_iterations_per_s=iters / (ms / 1e3),
                 evaluations_per_s=evals.value / (ms / 1e3),

@@ -97,56 +97,6 @@ __device__ __forceinline__ void prefetch_l2(const float* p, size_t n, int t) {
   }
 }
 
-// L2 eviction priority of a global access: normal, evict-first (the last use
-// of a streamed tape image) or evict-last (the reverse pass's working images).
-#ifndef WDL_X_HINTS
-#define WDL_X_HINTS 0
-#endif
-enum : int { kHN = 0, kHF = 1, kHL = 2 };
-template <int HINT>
-__device__ __forceinline__ uint64_t l2pol() {
-  uint64_t p;
-  if (HINT == kHF) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  else asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-template <int HINT>
-__device__ __forceinline__ float4 ldg4(const float* a) {
-  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) return __ldcg(reinterpret_cast<const float4*>(a));
-  float4 v;
-  asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "l"(a), "l"(l2pol<HINT>()));
-  return v;
-}
-template <int HINT>
-__device__ __forceinline__ float ldg1(const float* a) {
-  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) return __ldcg(a);
-  float v;
-  asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(l2pol<HINT>()));
-  return v;
-}
-template <int HINT>
-__device__ __forceinline__ void stg4(float* a, float4 v) {
-  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) { __stcg(reinterpret_cast<float4*>(a), v); return; }
-  asm volatile("st.global.cg.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "f"(v.x), "f"(v.y),
-               "f"(v.z), "f"(v.w), "l"(l2pol<HINT>())
-               : "memory");
-}
-template <int HINT>
-__device__ __forceinline__ void stg1(float* a, float v) {
-  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) { __stcg(a, v); return; }
-  asm volatile("st.global.cg.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(l2pol<HINT>()) : "memory");
-}
-// Hints of up to 4 inputs, 2 bits each.
-constexpr uint32_t hints(int a = kHN, int b = kHN, int c = kHN, int d = kHN) {
-  return (uint32_t)a | ((uint32_t)b << 2) | ((uint32_t)c << 4) | ((uint32_t)d << 6);
-}
-template <uint32_t HS, int A>
-struct HintOf {
-  static constexpr int v = (int)((HS >> (2 * A)) & 3u);
-};
-
 // Phase trace (thread 0 of a stream; only when a trace buffer is given):
 // claim, dependency wait, prologue, first convolution, mid, second
 // convolution, epilogue, completion; slot 8 counts items.
@@ -172,24 +122,23 @@ struct Geo {
   bool vec;
 };
 
-template <int NIN, int CE, uint32_t HS, int A>
+template <int NIN, int CE, int A>
 __device__ __forceinline__ void load_row_chunk(float (&in)[NIN > 0 ? NIN : 1][CE],
                                                const float* const (&src)[NIN > 0 ? NIN : 1], int i, int x0,
                                                bool row_ok, const Geo& g) {
   if constexpr (A < NIN) {
-    constexpr int H = HintOf<HS, A>::v;
     const float* row = src[A] + (size_t)i * g.W;
     if (row_ok && g.vec && x0 + CE <= g.W) {
 #pragma unroll
       for (int q = 0; q < CE; q += 4) {
-        const float4 f4 = ldg4<H>(row + x0 + q);
+        const float4 f4 = __ldcg(reinterpret_cast<const float4*>(row + x0 + q));
         in[A][q] = f4.x; in[A][q + 1] = f4.y; in[A][q + 2] = f4.z; in[A][q + 3] = f4.w;
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < CE; ++q) in[A][q] = (row_ok && x0 + q < g.W) ? ldg1<H>(row + x0 + q) : 0.f;
+      for (int q = 0; q < CE; ++q) in[A][q] = (row_ok && x0 + q < g.W) ? __ldcg(row + x0 + q) : 0.f;
     }
-    load_row_chunk<NIN, CE, HS, A + 1>(in, src, i, x0, row_ok, g);
+    load_row_chunk<NIN, CE, A + 1>(in, src, i, x0, row_ok, g);
   }
 }
 
@@ -197,7 +146,7 @@ __device__ __forceinline__ void load_row_chunk(float (&in)[NIN > 0 ? NIN : 1][CE
 // rows i < Hp, x < Wp (zero outside the H x W image).  UNR chunks of loads are
 // issued before any is consumed.  f may accumulate side sums (captured by
 // reference); it is only called for pixels inside the image.
-template <bool SPLIT, int NIN, uint32_t HS = 0, class F>
+template <bool SPLIT, int NIN, class F>
 __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
                                            F f, const Geo& g, int t) {
   constexpr int CE = SPLIT ? 8 : 4;
@@ -214,7 +163,7 @@ __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&s
       iu[u] = i;
       xu[u] = x0;
       const bool row_ok = c < total && i < g.H;
-      load_row_chunk<NIN, CE, HS, 0>(in[u], src, i, x0, row_ok, g);
+      load_row_chunk<NIN, CE, 0>(in[u], src, i, x0, row_ok, g);
     }
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
@@ -245,16 +194,8 @@ struct Ctl {
 // lane; warps w and w+4 of the stream take alternate 16-column chunks of the
 // same lanes) -> MMA2 (A from tensor memory, B = G) -> D2 in D1's columns.
 // Column form: K1 = Wp, N1 = Hp; row form: K1 = Hp, N1 = Wp.
-template <bool SPLIT, class PRE>
-__device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre);
 template <bool SPLIT>
 __device__ bool gemm_pair(Ctl& c, int K1, int N1) {
-  return gemm_pair<SPLIT>(c, K1, N1, [] {});
-}
-// The same, running pre() (loads that do not depend on the result) while the
-// first GEMM runs.
-template <bool SPLIT, class PRE>
-__device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre) {
   ptx::tc_fence_before();
   ptx::fence_proxy_async_smem();
   bar_sync(c.st, kSt);
@@ -263,7 +204,6 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre) {
     issue_gemm<SPLIT>(c.d1, c.g_a, c.x_a, K1, N1);
     ptx::mma_commit(c.bar_a);
   }
-  pre();
   bool ok = bar_all(ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt);
   c.phase ^= 1;
   ptx::tc_fence_after();
@@ -294,34 +234,26 @@ __device__ bool gemm_pair(Ctl& c, int K1, int N1, PRE pre) {
 // are loaded first (all loads in flight together), then m(idx, y, in) consumes
 // them (it may store) and returns the next operand's value, written as row x
 // (K = i) of the tile when stage_next.
-template <int NIN, uint32_t HS, int A>
+template <int NIN, int A>
 __device__ __forceinline__ void load_col_chunk(float (&in)[NIN][16], const float* const (&src)[NIN], int c0,
                                                int x, const Geo& g) {
   if constexpr (A < NIN) {
-    constexpr int H = HintOf<HS, A>::v;
 #pragma unroll
     for (int t = 0; t < 16; ++t) {
       const int i = c0 + t;
-      in[A][t] = (x < g.W && i < g.H) ? ldg1<H>(src[A] + (size_t)i * g.W + x) : 1.f;
+      in[A][t] = (x < g.W && i < g.H) ? __ldcg(src[A] + (size_t)i * g.W + x) : 1.f;
     }
-    load_col_chunk<NIN, HS, A + 1>(in, src, c0, x, g);
+    load_col_chunk<NIN, A + 1>(in, src, c0, x, g);
   }
 }
 
-template <bool SPLIT, int NIN, uint32_t HS = 0, class M>
+template <bool SPLIT, int NIN, class M>
 __device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
-                                            bool stage_next, const float (*first)[16] = nullptr) {
+                                            bool stage_next) {
   const int x = c.lane_row;
   for (int c0 = 16 * c.half; c0 < g.Hp; c0 += 32) {
     float in[NIN][16];
-    if (first && c0 == 16 * c.half) {  // this thread's first chunk, loaded during the GEMMs
-#pragma unroll
-      for (int q = 0; q < NIN; ++q)
-#pragma unroll
-        for (int t = 0; t < 16; ++t) in[q][t] = first[q][t];
-    } else {
-      load_col_chunk<NIN, HS, 0>(in, src, c0, x, g);
-    }
+    load_col_chunk<NIN, 0>(in, src, c0, x, g);
     float y[16];
     ptx::tmem_ld16(c.d2 + c.lane_base + (uint32_t)c0, y);
     ptx::tmem_ld_wait();
@@ -337,32 +269,23 @@ __device__ __forceinline__ void mid_columns(Ctl& c, const Geo& g, const float* c
   }
 }
 
-template <int NIN, uint32_t HS, int A>
+template <int NIN, int A>
 __device__ __forceinline__ void load_px4(float (&in)[NIN > 0 ? NIN : 1][4], const float* const (&src)[NIN > 0 ? NIN : 1],
                                          size_t idx, bool okr, int x0, const Geo& g) {
   if constexpr (A < NIN) {
-    constexpr int H = HintOf<HS, A>::v;
     if (okr && g.vec) {
-      const float4 f = ldg4<H>(src[A] + idx);
+      const float4 f = __ldcg(reinterpret_cast<const float4*>(src[A] + idx));
       in[A][0] = f.x; in[A][1] = f.y; in[A][2] = f.z; in[A][3] = f.w;
     } else {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) in[A][r] = (okr && x0 + r < g.W) ? ldg1<H>(src[A] + idx + r) : 1.f;
+      for (int r = 0; r < 4; ++r) in[A][r] = (okr && x0 + r < g.W) ? __ldcg(src[A] + idx + r) : 1.f;
     }
-    load_px4<NIN, HS, A + 1>(in, src, idx, okr, x0, g);
+    load_px4<NIN, A + 1>(in, src, idx, okr, x0, g);
   }
 }
 
-template <int HINT = kHN>
 __device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d) {
-  if (HINT == kHN || !WDL_X_HINTS || (WDL_X_HINTS == 1 && HINT == kHL)) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
-                 : "memory");
-  } else {
-    asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(a), "f"(b),
-                 "f"(c), "f"(d), "l"(l2pol<HINT>())
-                 : "memory");
-  }
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
 }
 __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x) : (float)kLogEpsilon; }
 
@@ -373,13 +296,9 @@ __device__ __forceinline__ float safe_logf(float x) { return x > 0.f ? __logf(x)
 // cover one row, so every global load, store and red is a contiguous 512-byte
 // row.  e(idx, y4, in4) gets 4 consecutive pixels, may store, and returns the
 // 4 values added into acc[idx..idx+3].
-#ifndef WDL_X_ROT
-#define WDL_X_ROT 0
-#endif
-template <int NIN, uint32_t HS = 0, int RH = kHN, class E>
+template <int NIN, class E>
 __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
-                                             float* acc, E e, int rot = 0,
-                                             const float (*first)[NIN > 0 ? NIN : 1][4] = nullptr) {
+                                             float* acc, E e) {
   {
     const int i = c.lane_row;
     uint8_t* rowp = c.tile + (size_t)i * 512;
@@ -405,26 +324,13 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
     int iu[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      int i = i0 + u * kWarps;
-#if WDL_X_ROT
-      // rows in an order rotated per atom, so that the K items reducing into
-      // the same image at the same time add into different rows
-      if (i < g.H) { i += rot; if (i >= g.H) i -= g.H; }
-      else i = g.H;
-#endif
+      const int i = i0 + u * kWarps;
       iu[u] = i;
       const bool okr = i < g.H && x0 < g.W;
       y4[u] = okr ? *reinterpret_cast<const float4*>(c.tile + (size_t)i * 512 + ((j ^ (i & 7)) << 4))
                   : make_float4(0.f, 0.f, 0.f, 0.f);
       const size_t idx = (size_t)i * g.W + x0;
-      if (first && i0 == (c.t >> 5)) {  // loaded during the GEMMs
-#pragma unroll
-        for (int q = 0; q < (NIN > 0 ? NIN : 1); ++q)
-#pragma unroll
-          for (int r = 0; r < 4; ++r) in[u][q][r] = first[u][q][r];
-      } else {
-        load_px4<NIN, HS, 0>(in[u], src, idx, okr, x0, g);
-      }
+      load_px4<NIN, 0>(in[u], src, idx, okr, x0, g);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -434,7 +340,7 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
       const int nv = g.W - x0 < 4 ? g.W - x0 : 4;
       const float4 out = e(idx, y4[u], in[u], nv);
       if (g.vec) {
-        red_add4<RH>(acc + idx, out.x, out.y, out.z, out.w);
+        red_add4(acc + idx, out.x, out.y, out.z, out.w);
       } else {
         const float o[4] = {out.x, out.y, out.z, out.w};
         for (int r = 0; r < nv; ++r) atomicAdd(acc + idx + r, o[r]);
@@ -443,28 +349,13 @@ __device__ __forceinline__ void epi_rows_red(Ctl& c, const Geo& g, const float* 
   }
 }
 
-// The inputs of the epilogue's first two rows for this thread (rows t/32 and
-// t/32 + 8, pixels 4 (t % 32) ..), for loading while the GEMMs run.
-template <int NIN, uint32_t HS>
-__device__ __forceinline__ void epi_first_loads(float (&pre)[2][NIN][4], const Ctl& c, const Geo& g,
-                                                const float* const (&src)[NIN]) {
-  const int x0 = 4 * (c.t & 31);
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    const int i = (c.t >> 5) + u * kWarps;
-    const bool okr = i < g.H && x0 < g.W;
-    load_px4<NIN, HS, 0>(pre[u], src, (size_t)i * g.W + x0, okr, x0, g);
-  }
-}
-
 // Stores 4 consecutive values (nv valid; 16-byte store when the row is aligned).
-template <int HINT = kHN>
 __device__ __forceinline__ void st4(float* p, float4 v, int nv, bool vec) {
   if (vec) {
-    stg4<HINT>(p, v);
+    __stcg(reinterpret_cast<float4*>(p), v);
   } else {
     const float o[4] = {v.x, v.y, v.z, v.w};
-    for (int r = 0; r < nv; ++r) stg1<HINT>(p + r, o[r]);
+    for (int r = 0; r < nv; ++r) __stcg(p + r, o[r]);
   }
 }
 
@@ -517,22 +408,11 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
   SkProblem* const pr = &s_prob[st];
   int cur_q = -1;
   Trace tr;
-#ifndef WDL_X_EARLY
-#define WDL_X_EARLY 0
-#endif
-#ifndef WDL_X_PREMID
-#define WDL_X_PREMID 0
-#endif
-#ifndef WDL_X_PREEPI
-#define WDL_X_PREEPI 0
-#endif
-  int next_item = -1;  // thread 0: the item claimed during the previous completion
   while (true) {
     tr.start(a.trace, t);
     tr.type = 0;
     if (t == 0) {
-      const int item = next_item >= 0 ? next_item : atomicAdd(work, 1);
-      next_item = -1;
+      const int item = atomicAdd(work, 1);
       int q = 0, type = 0, step = 0, pkv = 0;
       if (item < a.total) {
         if (a.items) {
@@ -635,7 +515,6 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     }
     tr.mark(1);
     const float lam = pr->lam[pk];
-    const int rot = WDL_X_ROT ? (k * g.H) / K : 0;
     const float* atom = pr->atoms + (size_t)k * N;
     bool ok = true;
 
@@ -666,19 +545,13 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       }
       tr.mark(2);
       const float* msrc[1] = {atom};
-#if WDL_X_PREMID
-      float pin[1][16];
-      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp, [&] { load_col_chunk<1, hints(kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
-#else
-      const float (*pin)[16] = nullptr;
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
-#endif
       tr.mark(3);
       const bool keep_cb = !fwd_only;
-      mid_columns<SPLIT, 1, hints(kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
-        if (keep_cb) stg1<kHF>(cb_out + idx, y);  // read again only in the reverse pass
+      mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
+        if (keep_cb) __stcg(cb_out + idx, y);  // read again only in the reverse pass
         return fdiv(in[0], y);
-      }, true, pin);
+      }, true);
       tr.mark(4);
       ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
       tr.mark(5);
@@ -689,55 +562,42 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         for (int r = 0; r < nv; ++r) bad |= !(o[r] > 0.f && o[r] <= FLT_MAX);
         return make_float4(lam * safe_logf(y.x), lam * safe_logf(y.y), lam * safe_logf(y.z),
                            lam * safe_logf(y.w));
-      }, rot);
+      });
       if (bad) *(volatile int*)(range + p) = 1;
       tr.mark(6);
     } else if (type == 1) {  // ---------------- reverse pass, dictionary recursion
       const int s = step;
       const float* src[4] = {pr->nb + (size_t)(s & 1) * PN + (size_t)p * N, pr->v + pk * N,
                              pr->acc + slot(s) * PN + (size_t)p * N, pr->phi + slot(s) * PKN + pk * N};
-      stage_rows<SPLIT, 4, hints(kHL, kHL, kHF, kHF)>(
+      stage_rows<SPLIT, 4>(
           c.tile, src, [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); }, g,
           t);
       tr.mark(2);
       const float* cbp = pr->cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
       float* gd = pr->gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
-#if WDL_X_PREMID
-      float pin[3][16];
-      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp,
-                            [&] { load_col_chunk<3, hints(kHF, kHL, kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
-#else
-      const float (*pin)[16] = nullptr;
       ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
-#endif
       tr.mark(3);
-      mid_columns<SPLIT, 3, hints(kHF, kHL, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
+      mid_columns<SPLIT, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
         const float rc = frcp(in[0]);
         const float q2 = y * rc;
-        stg1<kHL>(gd + idx, in[1] + q2);
+        __stcg(gd + idx, in[1] + q2);
         return -in[2] * q2 * rc;
-      }, s > 1, pin);
+      }, s > 1);
       tr.mark(4);
       if (s > 1) {
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
         const float* esrc[1] = {php};
-#if WDL_X_PREEPI && !WDL_X_ROT
-        float epre[2][1][4];
-        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp, [&] { epi_first_loads<1, hints(kHN)>(epre, c, g, esrc); });
-#else
-        const float (*epre)[1][4] = nullptr;
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
-#endif
         tr.mark(5);
         float* vout = pr->v + pk * N;
         float* nout = pr->nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        epi_rows_red<1, hints(kHN), kHL>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
+        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
           const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
                                         fdiv(y.w, in[0][3]));
-          st4<kHL>(vout + idx, vv, nv, g.vec);
+          st4(vout + idx, vv, nv, g.vec);
           return vv;
-        }, rot, epre);
+        });
         tr.mark(6);
       }
     } else {  // ---------------- reverse pass, weight recursion
@@ -745,7 +605,7 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       const float* src[3] = {pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N, pr->r + pk * N,
                              pr->phi + slot(s) * PKN + pk * N};
       double dacc = 0;
-      stage_rows<SPLIT, 3, hints(kHL, kHL, kHF)>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
+      stage_rows<SPLIT, 3>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
         dacc += (double)__logf(v[2]) * (double)v[0];
         return fdiv(lam * v[0] - v[1], v[2]);
       }, g, t);
@@ -755,41 +615,28 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
       if (s > 1) {
         const float* cbp = pr->cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
-#if WDL_X_PREMID
-        float pin[2][16];
-        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp,
-                              [&] { load_col_chunk<2, hints(kHF, kHL), 0>(pin, msrc, 16 * c.half, c.lane_row, g); });
-#else
-        const float (*pin)[16] = nullptr;
         ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
-#endif
         tr.mark(3);
-        mid_columns<SPLIT, 2, hints(kHF, kHL)>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
+        mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
           return y * (-in[1] * rc * rc);
-        }, true, pin);
+        }, true);
         tr.mark(4);
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
         const float* accp = pr->acc + slot(s - 1) * PN + (size_t)p * N;
         const float* esrc[2] = {accp, php};
-#if WDL_X_PREEPI && !WDL_X_ROT
-        float epre[2][2][4];
-        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp, [&] { epi_first_loads<2, hints(kHN, kHN)>(epre, c, g, esrc); });
-#else
-        const float (*epre)[2][4] = nullptr;
         ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
-#endif
         tr.mark(5);
         float* rout = pr->r + pk * N;
         float* gout = pr->gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        epi_rows_red<2, hints(kHN, kHN), kHL>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
+        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
           const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
                                         y.y * fdiv(__expf(in[0][1]), in[1][1]),
                                         y.z * fdiv(__expf(in[0][2]), in[1][2]),
                                         y.w * fdiv(__expf(in[0][3]), in[1][3]));
-          st4<kHL>(rout + idx, rr, nv, g.vec);
+          st4(rout + idx, rr, nv, g.vec);
           return rr;
-        }, rot, epre);
+        });
         tr.mark(6);
       }
     }
@@ -801,9 +648,6 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
     // Completion: the item that finishes a group publishes it.
     bar_sync(st, kSt);
     if (t == 0) {
-      // the next item's claim goes out before this item's release fence, so
-      // its round trip overlaps the fence and the completion count
-      if (WDL_X_EARLY) next_item = atomicAdd(work, 1);
       __threadfence();
       int fin;
       if (type == 0) fin = atomicAdd(&done_fwd[p], 1) + 1 == step * K;
@@ -851,8 +695,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
             const float q2 = bv / o32;
             gg = q2 > 0.f ? logf(q2) : (float)kLogEpsilon;
           }
-          if (dic) stg1<kHL>(n0 + j, gg);
-          stg1<kHL>(g0 + j, gg * bv);
+          if (dic) __stcg(n0 + j, gg);
+          __stcg(g0 + j, gg * bv);
         }
         const double tot = st_sum(lacc, s_dbl, st, t);
         if (t == 0) pr->loss[p] = lt == WDL_LOSS_TV ? 0.5 * tot : tot;
@@ -870,8 +714,8 @@ __global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a)
         float* zg = pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N;
         const bool dic = pr->need_dic != 0;
         for (size_t j = t; j < N; j += kSt) {
-          if (dic) stg1<kHL>(zn + j, 0.f);
-          stg1<kHL>(zg + j, 0.f);
+          if (dic) __stcg(zn + j, 0.f);
+          __stcg(zg + j, 0.f);
         }
       }
       bar_sync(st, kSt);
