@@ -32,7 +32,6 @@
 // K-major operand, so every SMEM write is a whole 16-byte chunk and every
 // global access of the epilogue is a contiguous row segment.
 #include <cfloat>
-#include <cstdlib>
 
 #include "tc_common.cuh"
 #include "wdl_math.cuh"
@@ -73,18 +72,15 @@ constexpr int kWarps = kSt / 32;
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ float frcp(float b) { return __fdividef(1.0f, b); }
 
-// Stream-wide sum of a double over a stream of NT threads (result valid in
-// every thread of the stream).
-template <int NT>
+// Stream-wide sum of a double (result valid in every thread of the stream).
 __device__ __forceinline__ double st_sum(double v, double* scratch, int st, int t) {
-  constexpr int NW = NT / 32;
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((t & 31) == 0) scratch[st * NW + (t >> 5)] = v;
-  bar_sync(st, NT);
+  if ((t & 31) == 0) scratch[st * kWarps + (t >> 5)] = v;
+  bar_sync(st, kSt);
   double tot = 0;
 #pragma unroll
-  for (int w = 0; w < NW; ++w) tot += scratch[st * NW + w];
-  bar_sync(st, NT);
+  for (int w = 0; w < kWarps; ++w) tot += scratch[st * kWarps + w];
+  bar_sync(st, kSt);
   return tot;
 }
 
@@ -150,23 +146,18 @@ __device__ __forceinline__ void load_row_chunk(float (&in)[NIN > 0 ? NIN : 1][CE
 // rows i < Hp, x < Wp (zero outside the H x W image).  UNR chunks of loads are
 // issued before any is consumed.  f may accumulate side sums (captured by
 // reference); it is only called for pixels inside the image.
-template <bool SPLIT, int NIN, int NT, class F>
+template <bool SPLIT, int NIN, class F>
 __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&src)[NIN > 0 ? NIN : 1],
                                            F f, const Geo& g, int t) {
   constexpr int CE = SPLIT ? 8 : 4;
-  // chunks in flight per thread: the three-stream form has half the threads
-  // per stream and more registers per thread
-#ifndef WDL_X_UNR3
-#define WDL_X_UNR3 2
-#endif
-  constexpr int UNR = NT == 256 ? (NIN > 2 ? 1 : 2) : (NIN > 2 ? WDL_X_UNR3 : 2);
+  constexpr int UNR = NIN > 2 ? 1 : 2;
   const int total = g.Hp * (int)g.cpr;
-  for (int base = t; base < total; base += NT * UNR) {
+  for (int base = t; base < total; base += kSt * UNR) {
     float in[UNR][NIN > 0 ? NIN : 1][CE];
     int iu[UNR], xu[UNR];
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
-      const int c = base + u * NT;
+      const int c = base + u * kSt;
       const int i = (int)__umulhi((uint32_t)c, g.cpr_magic);
       const int x0 = (c - i * (int)g.cpr) * CE;
       iu[u] = i;
@@ -176,7 +167,7 @@ __device__ __forceinline__ void stage_rows(uint8_t* tile, const float* const (&s
     }
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
-      if (base + u * NT >= total) break;
+      if (base + u * kSt >= total) break;
       const int i = iu[u], x0 = xu[u];
       float out[CE];
 #pragma unroll
@@ -368,211 +359,24 @@ __device__ __forceinline__ void st4(float* p, float4 v, int nv, bool vec) {
   }
 }
 
-// ---- the three-stream form ------------------------------------------------------
-// 3 streams x 4 warps per CTA.  The factor G stays in tensor memory as the A
-// operand of both GEMMs of a separable convolution (columns [0, 128): BF16 hi
-// [0, 64) and lo [64, 128), or TF32), which frees its 64 KB of SMEM for a third
-// operand tile; each stream owns one 64 KB tile and 128 TMEM columns.  With G
-// as A a GEMM keeps its operand's orientation — D[m][n] = sum_k G[m][k] T[n][k];
-// restaging D as the tile rows m (K = n) and multiplying by G again gives
-// G_rows T G_cols^T with lane = T's row index — so every convolution result is
-// in row form (lane = image row y, columns = x) and every elementwise step
-// works on rows: a thread owns one image row, reads and writes 16 consecutive
-// pixels per chunk with 16-byte accesses, and keeps the next chunk's loads in
-// flight while it works on the current one.  Three items per SM instead of two,
-// with 168 registers per thread for loads in flight instead of 128.
-constexpr int kSt3 = 128;
-
 template <bool SPLIT>
-__device__ bool conv_g(Ctl& c, int K1, int N1) {
-  ptx::tc_fence_before();
-  ptx::fence_proxy_async_smem();
-  bar_sync(c.st, kSt3);
-  if (c.t == 0) {
-    ptx::tc_fence_after();
-    issue_gemm_ta<SPLIT>(c.d1, c.a_hi, c.a_lo, c.x_a, K1, N1);
-    ptx::mma_commit(c.bar_a);
-  }
-  bool ok = bar_all(ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt3);
-  c.phase ^= 1;
-  ptx::tc_fence_after();
-  // D (lane m, columns n < N1) -> the tile as rows m < K1, K = n (whole
-  // 16-byte chunks of this thread's row); every thread of the warp takes part
-  // in the tensor-memory loads
-  const int m = c.lane_row;
-  for (int c0 = 0; c0 < N1; c0 += 16) {
-    float v[16];
-    ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, v);
-    ptx::tmem_ld_wait();
-    if (m < K1) put16<SPLIT>(c.tile, m, c0, v);
-  }
-  ptx::fence_proxy_async_smem();
-  ptx::tc_fence_before();
-  bar_sync(c.st, kSt3);
-  if (c.t == 0) {
-    ptx::tc_fence_after();
-    issue_gemm_ta<SPLIT>(c.d1, c.a_hi, c.a_lo, c.x_a, N1, K1);
-    ptx::mma_commit(c.bar_a);
-  }
-  ok = bar_all(ok && ptx::mbar_wait(c.bar_a, c.phase, kWaitNs), c.st, kSt3);
-  c.phase ^= 1;
-  ptx::tc_fence_after();
-  return ok;
-}
-
-// 16 values of row `rowoff`, pixels x0.. (x0 % 16 == 0) of each input, 1
-// outside the image.
-template <int NIN>
-__device__ __forceinline__ void load_row16(float (&in)[NIN][16], const float* const (&src)[NIN], size_t rowoff,
-                                           int x0, bool row_ok, const Geo& g) {
-#pragma unroll
-  for (int q = 0; q < NIN; ++q) {
-#pragma unroll
-    for (int e = 0; e < 16; e += 4) {
-      const int x = x0 + e;
-      if (row_ok && g.vec && x + 4 <= g.W) {
-        const float4 f = __ldcg(reinterpret_cast<const float4*>(src[q] + rowoff + x));
-        in[q][e] = f.x; in[q][e + 1] = f.y; in[q][e + 2] = f.z; in[q][e + 3] = f.w;
-      } else {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) in[q][e + r] = (row_ok && x + r < g.W) ? __ldcg(src[q] + rowoff + x + r) : 1.f;
-      }
-    }
-  }
-}
-
-// Row-form result (lane = row i): Y(i, x) chunk by chunk; m(idx, y, in)
-// consumes the NIN inputs at pixel idx = i*W + x (it may store) and returns
-// the next operand's value, written as row i (K = x) of the tile when
-// stage_next.  The next chunk's loads are issued before the current chunk is
-// worked on.
-template <bool SPLIT, int NIN, class M>
-__device__ __forceinline__ void mid_rows(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
-                                         bool stage_next) {
-  const int i = c.lane_row;
-  const bool row_ok = i < g.H;
-  const size_t rowoff = (size_t)i * g.W;
-  float a[NIN][16], b[NIN <= 2 ? NIN : 1][16];
-  auto work = [&](const float (&in)[NIN][16], int c0) {
-    float y[16];
-    ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, y);
-    ptx::tmem_ld_wait();
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const int x = c0 + t;
-      float iv[NIN];
-#pragma unroll
-      for (int q = 0; q < NIN; ++q) iv[q] = in[q][t];
-      y[t] = (row_ok && x < g.W) ? m(rowoff + x, y[t], iv) : 0.f;
-    }
-    if (stage_next && i < g.Hp) put16<SPLIT>(c.tile, i, c0, y);
-  };
-  if constexpr (NIN <= 2) {  // the next chunk's loads in flight during this chunk's work
-    load_row16<NIN>(a, src, rowoff, 0, row_ok, g);
-    for (int c0 = 0; c0 < g.Wp; c0 += 32) {
-      if (c0 + 16 < g.Wp) load_row16<NIN>(b, src, rowoff, c0 + 16, row_ok, g);
-      work(a, c0);
-      if (c0 + 16 >= g.Wp) break;
-      if (c0 + 32 < g.Wp) load_row16<NIN>(a, src, rowoff, c0 + 32, row_ok, g);
-      work(b, c0 + 16);
-    }
-  } else {  // three inputs: one chunk at a time (two would not fit the registers)
-    for (int c0 = 0; c0 < g.Wp; c0 += 16) {
-      load_row16<NIN>(a, src, rowoff, c0, row_ok, g);
-      work(a, c0);
-    }
-  }
-}
-
-// Row-form result with an accumulating epilogue: e(idx, y4, in4, nv) gets 4
-// consecutive pixels of this thread's row, may store, and returns the 4
-// values added into acc[idx..idx+3].
-template <int NIN, class E>
-__device__ __forceinline__ void epi_rows(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
-                                         float* acc, E e) {
-  constexpr int NI = NIN > 0 ? NIN : 1;
-  const int i = c.lane_row;
-  const bool row_ok = i < g.H;
-  const size_t rowoff = (size_t)i * g.W;
-  float a[NI][16];
-  auto load = [&](float (&in)[NI][16], int x0) {
-    if constexpr (NIN > 0) load_row16<NIN>(in, src, rowoff, x0, row_ok, g);
-  };
-  auto work = [&](const float (&in)[NI][16], int c0) {
-    float y[16];
-    ptx::tmem_ld16(c.d1 + c.lane_base + (uint32_t)c0, y);
-    ptx::tmem_ld_wait();
-#pragma unroll
-    for (int q4 = 0; q4 < 4; ++q4) {
-      const int x0 = c0 + 4 * q4;
-      if (!row_ok || x0 >= g.W) continue;
-      const int nv = g.W - x0 < 4 ? g.W - x0 : 4;
-      float in4[NI][4];
-#pragma unroll
-      for (int q = 0; q < NI; ++q)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) in4[q][r] = in[q][4 * q4 + r];
-      const size_t idx = rowoff + x0;
-      const float4 out = e(idx, make_float4(y[4 * q4], y[4 * q4 + 1], y[4 * q4 + 2], y[4 * q4 + 3]), in4, nv);
-      if (g.vec) {
-        red_add4(acc + idx, out.x, out.y, out.z, out.w);
-      } else {
-        const float o[4] = {out.x, out.y, out.z, out.w};
-        for (int r = 0; r < nv; ++r) atomicAdd(acc + idx + r, o[r]);
-      }
-    }
-  };
-  for (int c0 = 0; c0 < g.Wp; c0 += 16) {
-    load(a, c0);
-    work(a, c0);
-  }
-}
-
-// The phases of an item in either form (DS: streams per CTA).
-template <bool SPLIT, int DS>
-__device__ __forceinline__ bool conv_first(Ctl& c, const Geo& g) {
-  if constexpr (DS == 2) return gemm_pair<SPLIT>(c, g.Wp, g.Hp);  // column form
-  else return conv_g<SPLIT>(c, g.Wp, g.Hp);
-}
-template <bool SPLIT, int DS>
-__device__ __forceinline__ bool conv_second(Ctl& c, const Geo& g) {
-  if constexpr (DS == 2) return gemm_pair<SPLIT>(c, g.Hp, g.Wp);  // row form
-  else return conv_g<SPLIT>(c, g.Wp, g.Hp);
-}
-template <bool SPLIT, int DS, int NIN, class M>
-__device__ __forceinline__ void mid_phase(Ctl& c, const Geo& g, const float* const (&src)[NIN], M m,
-                                          bool stage_next) {
-  if constexpr (DS == 2) mid_columns<SPLIT, NIN>(c, g, src, m, stage_next);
-  else mid_rows<SPLIT, NIN>(c, g, src, m, stage_next);
-}
-template <int DS, int NIN, class E>
-__device__ __forceinline__ void epi_phase(Ctl& c, const Geo& g, const float* const (&src)[NIN > 0 ? NIN : 1],
-                                          float* acc, E e) {
-  if constexpr (DS == 2) epi_rows_red<NIN>(c, g, src, acc, e);
-  else epi_rows<NIN>(c, g, src, acc, e);
-}
-
-template <bool SPLIT, int DS>
-__global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(const SkArgs a) {
-  constexpr int NT = DS == 2 ? 256 : kSt3;  // threads of one stream
-  constexpr int NW = NT / 32;
+__global__ void __launch_bounds__(2 * kSt, 1) sinkhorn_tc_kernel(const SkArgs a) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int st = warp / NW, t = tid % NT, ws = warp % NW;
-  // SMEM: three 64 KB tiles (the two-stream form: G and two operand tiles; the
-  // three-stream form: three operand tiles), then the control block
-  uint8_t* ctl = base + 3 * kTileBytes;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ctl);                 // [3]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ctl + 32);
-  int* s_int = reinterpret_cast<int*>(ctl + 64);                     // [3][4]
-  double* s_dbl = reinterpret_cast<double*>(ctl + 128);              // [3 * 4 or 2 * 8]
-  SkProblem* s_prob = reinterpret_cast<SkProblem*>(ctl + 256);       // [DS]
+  const int st = warp / kWarps, t = tid % kSt, ws = warp % kWarps;
+  uint8_t* g_tile = base;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 3 * kTileBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + 3 * kTileBytes + 16);
+  int* s_int = reinterpret_cast<int*>(base + 3 * kTileBytes + 32);          // [2][4]
+  double* s_dbl = reinterpret_cast<double*>(base + 3 * kTileBytes + 64);    // [2][kWarps]
+  SkProblem* s_prob = reinterpret_cast<SkProblem*>(base + 3 * kTileBytes + 256);  // [2]
 
-  if constexpr (DS == 2) load_factor<SPLIT>(base, a.G, a.Gn, tid, blockDim.x);
+  load_factor<SPLIT>(g_tile, a.G, a.Gn, tid, blockDim.x);
   if (tid == 0) {
-    for (int q = 0; q < DS; ++q) ptx::mbar_init(ptx::smem_addr(&bars[q]), 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[0]), 1);
+    ptx::mbar_init(ptx::smem_addr(&bars[1]), 1);
     ptx::fence_mbar_init();
   }
   if (warp == 0) ptx::tmem_alloc(ptx::smem_addr(tmem_slot), 2 * kTmemCols);
@@ -580,53 +384,24 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
   ptx::tc_fence_before();
   __syncthreads();
   ptx::tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  if constexpr (DS == 3) {
-    // G into tensor memory as the A operand: row m (lane m) by warps 0..3,
-    // BF16 hi at columns [0, 64) and lo at [64, 128), or TF32 at [0, 128)
-    if (warp < 4) {
-      const int m = warp * 32 + lane;
-      for (int c0 = 0; c0 < kRows; c0 += 16) {
-        float v[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q)
-          v[q] = (m < a.Gn && c0 + q < a.Gn) ? a.G[(size_t)m * a.Gn + c0 + q] : 0.f;
-        restage16_tmem<SPLIT>(tmem, tmem + 64, (uint32_t)(warp * 32) << 16, c0, v);
-      }
-      ptx::tmem_st_wait();
-    }
-    ptx::tc_fence_before();
-    __syncthreads();
-    ptx::tc_fence_after();
-  }
 
   Ctl c;
+  c.tile = base + (1 + st) * kTileBytes;
+  c.g_a = ptx::smem_addr(g_tile);
+  c.x_a = ptx::smem_addr(c.tile);
   c.bar_a = ptx::smem_addr(&bars[st]);
+  // per stream: D1 and D2 share columns [0, 128), the second GEMM's A operand
+  // in tensor memory takes [128, 256) (BF16 hi [128, 192), lo [192, 256))
+  c.d1 = *tmem_slot + (uint32_t)st * kTmemCols;
+  c.d2 = c.d1;
+  c.a_hi = c.d1 + 128;
+  c.a_lo = c.d1 + 192;
+  c.lane_base = (uint32_t)((ws & 3) * 32) << 16;
   c.st = st;
   c.t = t;
+  c.lane_row = (ws & 3) * 32 + lane;
+  c.half = ws >> 2;
   c.phase = 0;
-  if constexpr (DS == 2) {
-    c.tile = base + (1 + st) * kTileBytes;
-    c.g_a = ptx::smem_addr(base);
-    // per stream: D1 and D2 share columns [0, 128), the second GEMM's A operand
-    // in tensor memory takes [128, 256) (BF16 hi [128, 192), lo [192, 256))
-    c.d1 = tmem + (uint32_t)st * kTmemCols;
-    c.a_hi = c.d1 + 128;
-    c.a_lo = c.d1 + 192;
-    c.lane_row = (ws & 3) * 32 + lane;
-    c.half = ws >> 2;
-  } else {
-    c.tile = base + st * kTileBytes;
-    c.g_a = 0;
-    c.d1 = tmem + 128 + (uint32_t)st * 128;  // D; G is the A operand at [0, 128)
-    c.a_hi = tmem;
-    c.a_lo = tmem + 64;
-    c.lane_row = ws * 32 + lane;
-    c.half = 0;
-  }
-  c.d2 = c.d1;
-  c.x_a = ptx::smem_addr(c.tile);
-  c.lane_base = (uint32_t)((ws & 3) * 32) << 16;
 
   int* work = a.sync;
   int* err = a.sync + 1;
@@ -665,7 +440,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       s_int[st * 4 + 2] = step;
       s_int[st * 4 + 3] = pkv;
     }
-    bar_sync(st, NT);
+    bar_sync(st, kSt);
     const int q = s_int[st * 4];
     if (q < 0) break;
     const int type = s_int[st * 4 + 1], step = s_int[st * 4 + 2];
@@ -675,7 +450,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       if (t < nw) reinterpret_cast<uint32_t*>(pr)[t] = reinterpret_cast<const uint32_t*>(&a.probs[q])[t];
       cur_q = q;
     }
-    bar_sync(st, NT);
+    bar_sync(st, kSt);
     tr.type = type;
     const int K = pr->K, L = pr->L, P = pr->P;
     const size_t N = pr->N, PN = (size_t)P * N, PKN = (size_t)P * K * N;
@@ -733,7 +508,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       }
       s_int[st * 4 + 1] = ok ? 1 : 0;
     }
-    bar_sync(st, NT);
+    bar_sync(st, kSt);
     if (!s_int[st * 4 + 1]) {
       if (t == 0) atomicExch(err, WDL_ERR_TIMEOUT);
       break;
@@ -758,30 +533,30 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       if (it == 1) {
         if (pr->b0) {
           const float* src[1] = {pr->b0 + pk * N};
-          stage_rows<SPLIT, 1, NT>(c.tile, src, [](const float (&v)[1]) { return v[0]; }, g, t);
+          stage_rows<SPLIT, 1>(c.tile, src, [](const float (&v)[1]) { return v[0]; }, g, t);
         } else {
           const float* src[1] = {atom};
-          stage_rows<SPLIT, 0, NT>(c.tile, src, [](const float (&)[1]) { return 1.f; }, g, t);
+          stage_rows<SPLIT, 0>(c.tile, src, [](const float (&)[1]) { return 1.f; }, g, t);
         }
       } else {  // b[it-1] = exp(acc[it-1]) / phi[it-1]
         const float* src[2] = {pr->acc + slot(it - 1) * PN + (size_t)p * N,
                                pr->phi + slot(it - 1) * PKN + pk * N};
-        stage_rows<SPLIT, 2, NT>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
+        stage_rows<SPLIT, 2>(c.tile, src, [](const float (&v)[2]) { return fdiv(__expf(v[0]), v[1]); }, g, t);
       }
       tr.mark(2);
       const float* msrc[1] = {atom};
-      ok = conv_first<SPLIT, DS>(c, g);
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
       tr.mark(3);
       const bool keep_cb = !fwd_only;
-      mid_phase<SPLIT, DS, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
+      mid_columns<SPLIT, 1>(c, g, msrc, [&](size_t idx, float y, const float (&in)[1]) {
         if (keep_cb) __stcg(cb_out + idx, y);  // read again only in the reverse pass
         return fdiv(in[0], y);
       }, true);
       tr.mark(4);
-      ok = ok && conv_second<SPLIT, DS>(c, g);
+      ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
       tr.mark(5);
       const float* esrc[1] = {nullptr};
-      epi_phase<DS, 0>(c, g, esrc, acc_out, [&](size_t idx, float4 y, const float (&)[1][4], int nv) {
+      epi_rows_red<0>(c, g, esrc, acc_out, [&](size_t idx, float4 y, const float (&)[1][4], int nv) {
         st4(phi_out + idx, y, nv, g.vec);
         const float o[4] = {y.x, y.y, y.z, y.w};
         for (int r = 0; r < nv; ++r) bad |= !(o[r] > 0.f && o[r] <= FLT_MAX);
@@ -794,16 +569,16 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       const int s = step;
       const float* src[4] = {pr->nb + (size_t)(s & 1) * PN + (size_t)p * N, pr->v + pk * N,
                              pr->acc + slot(s) * PN + (size_t)p * N, pr->phi + slot(s) * PKN + pk * N};
-      stage_rows<SPLIT, 4, NT>(
+      stage_rows<SPLIT, 4>(
           c.tile, src, [lam](const float (&v)[4]) { return (lam * v[0] - v[1]) * fdiv(__expf(v[2]), v[3]); }, g,
           t);
       tr.mark(2);
       const float* cbp = pr->cb + slot(s) * PKN + pk * N;  // cb[s-1] sits in slot(s)
       float* gd = pr->gdic + pk * N;
       const float* msrc[3] = {cbp, gd, atom};
-      ok = conv_first<SPLIT, DS>(c, g);
+      ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
       tr.mark(3);
-      mid_phase<SPLIT, DS, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
+      mid_columns<SPLIT, 3>(c, g, msrc, [&](size_t idx, float y, const float (&in)[3]) {
         const float rc = frcp(in[0]);
         const float q2 = y * rc;
         __stcg(gd + idx, in[1] + q2);
@@ -813,11 +588,11 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       if (s > 1) {
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
         const float* esrc[1] = {php};
-        ok = ok && conv_second<SPLIT, DS>(c, g);
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
         tr.mark(5);
         float* vout = pr->v + pk * N;
         float* nout = pr->nb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        epi_phase<DS, 1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
+        epi_rows_red<1>(c, g, esrc, nout, [&](size_t idx, float4 y, const float (&in)[1][4], int nv) {
           const float4 vv = make_float4(fdiv(y.x, in[0][0]), fdiv(y.y, in[0][1]), fdiv(y.z, in[0][2]),
                                         fdiv(y.w, in[0][3]));
           st4(vout + idx, vv, nv, g.vec);
@@ -830,19 +605,19 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       const float* src[3] = {pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N, pr->r + pk * N,
                              pr->phi + slot(s) * PKN + pk * N};
       double dacc = 0;
-      stage_rows<SPLIT, 3, NT>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
+      stage_rows<SPLIT, 3>(c.tile, src, [lam, &dacc](const float (&v)[3]) {
         dacc += (double)__logf(v[2]) * (double)v[0];
         return fdiv(lam * v[0] - v[1], v[2]);
       }, g, t);
-      const double dsum = st_sum<NT>(dacc, s_dbl, st, t);
+      const double dsum = st_sum(dacc, s_dbl, st, t);
       if (t == 0) atomicAdd(&pr->dot[pk], dsum);
       tr.mark(2);
       if (s > 1) {
         const float* cbp = pr->cb + slot(s) * PKN + pk * N;
         const float* msrc[2] = {cbp, atom};
-        ok = conv_first<SPLIT, DS>(c, g);
+        ok = gemm_pair<SPLIT>(c, g.Wp, g.Hp);
         tr.mark(3);
-        mid_phase<SPLIT, DS, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
+        mid_columns<SPLIT, 2>(c, g, msrc, [&](size_t idx, float y, const float (&in)[2]) {
           const float rc = frcp(in[0]);
           return y * (-in[1] * rc * rc);
         }, true);
@@ -850,11 +625,11 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
         const float* php = pr->phi + slot(s - 1) * PKN + pk * N;
         const float* accp = pr->acc + slot(s - 1) * PN + (size_t)p * N;
         const float* esrc[2] = {accp, php};
-        ok = ok && conv_second<SPLIT, DS>(c, g);
+        ok = ok && gemm_pair<SPLIT>(c, g.Hp, g.Wp);
         tr.mark(5);
         float* rout = pr->r + pk * N;
         float* gout = pr->gwb + (size_t)((s - 1) & 1) * PN + (size_t)p * N;
-        epi_phase<DS, 2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
+        epi_rows_red<2>(c, g, esrc, gout, [&](size_t idx, float4 y, const float (&in)[2][4], int nv) {
           const float4 rr = make_float4(y.x * fdiv(__expf(in[0][0]), in[1][0]),
                                         y.y * fdiv(__expf(in[0][1]), in[1][1]),
                                         y.z * fdiv(__expf(in[0][2]), in[1][2]),
@@ -871,7 +646,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
     }
 
     // Completion: the item that finishes a group publishes it.
-    bar_sync(st, NT);
+    bar_sync(st, kSt);
     if (t == 0) {
       __threadfence();
       int fin;
@@ -879,7 +654,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
       else fin = atomicAdd(&done_bwd[p], 1) + 1 == (pr->need_dic ? 2 : 1) * K * (L - step + 1);
       s_int[st * 4 + 2] = fin;
     }
-    bar_sync(st, NT);
+    bar_sync(st, kSt);
     if (!s_int[st * 4 + 2]) {
       tr.mark(7);
       if (tr.buf) atomicAdd(&tr.buf[type * 9 + 8], 1ull);
@@ -892,7 +667,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
         // acc[it-1] has been read by every item of iteration it: clear its slot,
         // which iteration it+1 accumulates into.
         float* z = pr->acc + slot(it + 1) * PN + (size_t)p * N;
-        for (size_t j = t; j < N; j += NT) __stcg(z + j, 0.f);
+        for (size_t j = t; j < N; j += kSt) __stcg(z + j, 0.f);
       }
       const bool last = it == L && !fwd_only;
       if (last) {  // loss and its gradient (cpp/loss.h:19-90); messages for s = L
@@ -902,7 +677,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
         const bool dic = pr->need_dic != 0;
         const int lt = pr->loss_type;
         double lacc = 0;
-        for (size_t j = t; j < N; j += NT) {
+        for (size_t j = t; j < N; j += kSt) {
           const float bv = expf(__ldcg(accL + j));
           const double o = pr->obs[(size_t)p * N + j];
           const float o32 = (float)o;
@@ -923,10 +698,10 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
           if (dic) __stcg(n0 + j, gg);
           __stcg(g0 + j, gg * bv);
         }
-        const double tot = st_sum<NT>(lacc, s_dbl, st, t);
+        const double tot = st_sum(lacc, s_dbl, st, t);
         if (t == 0) pr->loss[p] = lt == WDL_LOSS_TV ? 0.5 * tot : tot;
       }
-      bar_sync(st, NT);
+      bar_sync(st, kSt);
       if (t == 0) {
         __threadfence();
         st_release(&bary_ready[p], it);
@@ -938,12 +713,12 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
         float* zn = pr->nb + (size_t)(s & 1) * PN + (size_t)p * N;
         float* zg = pr->gwb + (size_t)(s & 1) * PN + (size_t)p * N;
         const bool dic = pr->need_dic != 0;
-        for (size_t j = t; j < N; j += NT) {
+        for (size_t j = t; j < N; j += kSt) {
           if (dic) __stcg(zn + j, 0.f);
           __stcg(zg + j, 0.f);
         }
       }
-      bar_sync(st, NT);
+      bar_sync(st, kSt);
       if (t == 0) {
         __threadfence();
         st_release(&msg_ready[p], L - s + 1);
@@ -954,7 +729,7 @@ __global__ void __launch_bounds__(DS == 2 ? 512 : 384, 1) sinkhorn_tc_kernel(con
   }
   __syncthreads();
   ptx::tc_fence_after();
-  if (warp == 0) ptx::tmem_dealloc(tmem, 2 * kTmemCols);
+  if (warp == 0) ptx::tmem_dealloc(*tmem_slot, 2 * kTmemCols);
 }
 
 // Histograms whose forward pass flagged scalings beyond the FP32 range
@@ -1022,32 +797,17 @@ double sk_problem_applications(const SkProblem& pr) {
   return PK * (2 * L + (pr.need_dic ? 2 * L - 1 : 0) + 2 * (L - 1));
 }
 
-// Streams per CTA of the fused kernel: 2 (factor in SMEM, column / row forms)
-// unless WDL_FUSED_STREAMS=3 selects the three-stream form.
-int fused_streams() {
-  static const int n = [] {
-    const char* e = std::getenv("WDL_FUSED_STREAMS");
-    return e && std::atoi(e) == 3 ? 3 : 2;
-  }();
-  return n;
-}
-
-template <bool SPLIT, int DS>
-int sk_launch_form(wdl_ctx* ctx, const SkArgs& a, cudaStream_t s) {
-  const size_t smem = 3 * tc::kTileBytes + 1024 + 256 + 3 * sizeof(SkProblem) + 64;
-  WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<SPLIT, DS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-  const long long streams = (a.total + DS - 1) / DS;
-  const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
-  sinkhorn_tc_kernel<SPLIT, DS><<<grid, DS == 2 ? 512 : 384, smem, s>>>(a);
-  WDL_LAUNCH_CHECK(ctx);
-  return WDL_OK;
-}
-
 int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
+  const size_t smem = 3 * tc::kTileBytes + 1024 + 256 + 2 * sizeof(SkProblem) + 64;
   const bool split = ctx->precision == WDL_SPLIT_BF16;
   k_sync_init<<<a.nprobs < 256 ? a.nprobs : 256, 128, 0, s>>>(a.sync, a.probs, a.nprobs);
   WDL_LAUNCH_CHECK(ctx);
+  if (split)
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  else
+    WDL_CUDA_TRY(ctx, cudaFuncSetAttribute(sinkhorn_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long streams = (a.total + 1) / 2;
+  const unsigned grid = (unsigned)(streams < ctx->sm_count ? streams : ctx->sm_count);
   a.trace = nullptr;
   a.dep_wait_ns = ctx->wait_limit_s > 0 ? (unsigned long long)(ctx->wait_limit_s * 1e9) : kDepWaitNs;
   if (ctx->trace_level >= 2) {
@@ -1056,12 +816,9 @@ int sinkhorn_tc_launch(wdl_ctx* ctx, SkArgs& a, cudaStream_t s) {
     a.trace = ctx->d_trace;
   }
   if (ctx->profiling) cudaEventRecord(ctx->ev_a, s);
-  int rc;
-  if (fused_streams() == 3)
-    rc = split ? sk_launch_form<true, 3>(ctx, a, s) : sk_launch_form<false, 3>(ctx, a, s);
-  else
-    rc = split ? sk_launch_form<true, 2>(ctx, a, s) : sk_launch_form<false, 2>(ctx, a, s);
-  if (rc) return rc;
+  if (split) sinkhorn_tc_kernel<true><<<grid, 2 * kSt, smem, s>>>(a);
+  else sinkhorn_tc_kernel<false><<<grid, 2 * kSt, smem, s>>>(a);
+  WDL_LAUNCH_CHECK(ctx);
   k_poison_flagged<<<a.nprobs < 256 ? a.nprobs : 256, 256, 0, s>>>(a.probs, a.nprobs);
   WDL_LAUNCH_CHECK(ctx);
   if (ctx->profiling) {
