@@ -343,8 +343,7 @@ def run_ours(args):
                                   tile_rows=choice.value, ms=round(tms.value, 4)))
             else:  # log-domain axis pass: rows per block
                 tuned.append(dict(kind="log_axis_pass", rows=key6[1], row_len=key6[2], images=key6[3],
-                                  signed=bool(key6[5]), rows_per_block=choice.value % 100,
-                                  layout="warp per row" if choice.value >= 100 else "rows fastest",
+                                  signed=bool(key6[5]), rows_per_block=choice.value,
                                   ms=round(tms.value, 4)))
     peaks = {}
     try:

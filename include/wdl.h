@@ -284,8 +284,7 @@ int wdl_conv_profile(const wdl_ctx* ctx, double* conv_ms, long long* conv_launch
                      double* conv_images);
 /* Launch shapes the autotuner chose on this context: entry i has key {kind,
  * rows, row length, images, element bytes, signed} (kind 1 = log-domain axis
- * pass: variant = rows per block, plus 100 for the layout with one warp per
- * row; kind 2 = tensor-core axis pass: variant =
+ * pass: variant = rows per block; kind 2 = tensor-core axis pass: variant =
  * output tile height, element bytes 2 for split BF16 and 4 for TF32), the
  * chosen variant and its time in ms.  wdl_autotune_count returns the number of
  * entries.  wdl_set_autotune(ctx, 0) stops this context from timing variants

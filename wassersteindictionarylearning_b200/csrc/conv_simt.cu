@@ -109,28 +109,33 @@ int axis_pass(wdl_ctx* ctx, const T* in, T* out, const T* G, int R, int C, size_
 }
 
 // ---- log-domain axis pass ---------------------------------------------------------
-// out[c][r] = log sum_k s_k exp(-(c-k)^2/gamma + in[r][k]) with the reference's
-// two passes per output: the maximum of the exponents, then the shifted sum
-// (cpp/kernels.h:1082-1091).  With signs, s_k = +-1 from in_sign and the sign of
-// the sum goes to out_sign, log|sum| to out (cpp/kernels.h:1123-1136).
+// out[c][r] = log sum_k s_k exp(-(c-k)^2/gamma + in[r][k]), the reference's
+// stabilised log-sum-exp (cpp/kernels.h:1082-1091).  With signs, s_k = +-1 from
+// in_sign and the sign of the sum goes to out_sign, log|sum| to out
+// (cpp/kernels.h:1123-1136).  The reference takes the maximum of the exponents
+// in one pass and the shifted sum in a second; here the two are one pass with
+// the running maximum (a new maximum rescales the partial sum), which gives the
+// same value to rounding.
 //
-// A block owns LR rows of one image (staged in SMEM with an odd row stride, so
-// the rows a warp reads at one tap fall in different banks) and produces every
-// output of those rows.  Taps are visited outwards from k = c, both sides per
-// step.  With X = max_k in[r][k], every tap at distance >= d has exponent
-// <= -d^2/gamma + X, so:
-//  * the maximum pass stops at the first d where -d^2/gamma + X <= max so far;
-//  * the sum pass stops at the first d where -d^2/gamma + X < max - kTail; the
-//    taps left out add at most 2C e^-kTail relative to the largest term, below
-//    the rounding of the sum (kTail = 40 bits for FP32, 60 nats for FP64), so
-//    the result is the full sum's to rounding.
-// FP32 works in base 2 (inputs scaled by log2 e once when staged; ex2 / lg2),
-// FP64 in base e with exp / log.  The summation order (outwards, both sides)
-// differs from the reference's k = 0..C-1; only rounding depends on it.  LR
-// (rows per block) is chosen per shape by the autotuner below; every output is
-// computed by the same operations whatever LR is, so the choice never changes
-// a result.
-constexpr int kLogRowsDefault = 16;
+// A block owns LR rows of one image, staged in SMEM with an odd row stride (the
+// rows of a warp fall in different banks).  A thread makes four neighbouring
+// outputs c0..c0+3 of one row (c0 a multiple of 4): taps go outwards from the
+// centres, both sides per step, and one step at distance d needs only two new
+// row values (in[c0 - d] and in[c0 + 3 + d]; the other six taps of the step are
+// values the four outputs have read at earlier steps), one tap weight and one
+// stop test for the four.  With X = max_k in[r][k], every tap at distance >= d
+// has exponent <= -d^2/gamma + X, so the group stops at the first d where
+// -d^2/gamma + X < max - kTail for each of its outputs: the taps left out add at
+// most 2C e^-kTail relative to an output's largest term, below the rounding of
+// its sum (kTail = 40 bits for FP32, 60 nats for FP64).  FP32 works in base 2
+// (inputs scaled by log2 e once when staged; ex2 / lg2), FP64 in base e with
+// exp / log.  The summation order (centre, then outwards, both sides) differs
+// from the reference's k = 0..C-1; only rounding depends on it.
+//
+// An output's result depends only on its row and its group (fixed by c), never
+// on the block shape: LR (rows per block) is chosen per shape by the autotuner
+// below without changing a result.
+constexpr int kLogRowsDefault = 32;
 
 template <typename T>
 struct LogOps;
@@ -139,9 +144,11 @@ struct LogOps<float> {
   static constexpr float kScale = 1.4426950408889634f;   // log2 e: natural -> base 2
   static constexpr float kUnscale = 0.6931471805599453f;  // ln 2
   static constexpr float kTail = 40.f;                   // bits
-  static constexpr float kFloor = -3.402823466e38f;      // start of the maximum
-  // the hardware base-2 exponential; arguments are <= 0 here and results
-  // below 2^-126 are far under the sum's rounding, so flushing them is exact
+  static constexpr float kFloor = -3.402823466e38f;      // lowest start of a maximum
+  static constexpr float kNone = -__builtin_huge_valf();  // a tap outside the row
+  // the hardware base-2 exponential; arguments are <= 0 here (up to rounding)
+  // and results below 2^-126 are far under the sum's rounding, so flushing them
+  // is exact
   __device__ static float ex(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -161,88 +168,200 @@ struct LogOps<double> {
   static constexpr double kUnscale = 1.0;
   static constexpr double kTail = 60.0;   // nats
   static constexpr double kFloor = -1e99;  // the reference's start (cpp/kernels.h:1083)
+  static constexpr double kNone = -__builtin_huge_val();
   __device__ static double ex(double x) { return exp(x); }
   __device__ static double lg(double x) { return log(x); }
 };
 
-// One output of the log-domain pass: out = log |sum_k s_k exp(lk[|c-k|] + row[k])|
-// (in the kernel's base) and its sign, by the two passes described above.  Both
-// kernel layouts below call this, so an output's arithmetic does not depend on
-// the layout.  *taps receives the number of exponentials evaluated.
-template <typename T, bool SIGNED>
-__device__ __forceinline__ T log_out(const T* __restrict__ row, const uint8_t* __restrict__ sgn,
-                                     const T* __restrict__ lk, T X, int c, int C, bool* pos, unsigned* taps) {
+// The state of one group of four outputs: running maxima m[j] and sums s[j],
+// and the taps of the current step in two 4-entry rings indexed by row
+// position mod 4 (left taps in lq, right taps in rq; their signs as +-1 in lsg
+// and rsg).  At distance d output j reads lq[(j - d) & 3] and rq[(j + d) & 3].
+template <typename T>
+struct LogGroup {
+  T m[4], s[4];
+  T lq[4], rq[4];
+  T lsg[4], rsg[4];
+  T mtail;  // min over the group's outputs of m - kTail
+  int nv;   // outputs of the group inside the row
+};
+
+template <typename T>
+__device__ __forceinline__ void log_group_mtail(LogGroup<T>& g) {
+  T mn = g.m[0];
+#pragma unroll
+  for (int j = 1; j < 4; ++j)
+    if (j < g.nv) mn = g.m[j] < mn ? g.m[j] : mn;
+  g.mtail = mn - LogOps<T>::kTail;
+}
+
+// One step at distance d (d & 3 == DM, d >= 2); false once the group is done.
+template <typename T, bool SIGNED, int DM>
+__device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restrict__ row,
+                                               const uint8_t* __restrict__ sgn, const T* __restrict__ lk,
+                                               T X, int c0, int C, int d, int dend) {
   using Op = LogOps<T>;
-  const int dboth = min(c, C - 1 - c);      // both sides inside the row for d <= dboth
-  const int sgnd = c < C - 1 - c ? 1 : -1;  // the side that remains beyond dboth
-  T m = row[c] > Op::kFloor ? row[c] : Op::kFloor;
-  int d = 1;
-  for (; d <= dboth; ++d) {
-    const T l = lk[d];
-    if (l + X <= m) break;
-    const T a = l + row[c - d], b = l + row[c + d];
-    const T ab = a > b ? a : b;
-    m = ab > m ? ab : m;
-  }
-  if (d > dboth) {
-    for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
-      const T l = lk[d];
-      if (l + X <= m) break;
-      const T t = l + row[c + sgnd * d];
-      m = t > m ? t : m;
-    }
-  }
-  T sum = Op::ex(row[c] - m);
-  if (SIGNED && !sgn[c]) sum = -sum;
-  const T fl = m - Op::kTail;
-  for (d = 1; d <= dboth; ++d) {
-    const T l = lk[d];
-    if (l + X < fl) break;
-    const T lm = l - m;
-    const T ea = Op::ex(lm + row[c - d]), eb = Op::ex(lm + row[c + d]);
-    if (SIGNED) sum += (sgn[c - d] ? ea : -ea) + (sgn[c + d] ? eb : -eb);
-    else sum += ea + eb;
-  }
-  if (d > dboth) {
-    for (; d < C && (sgnd > 0 ? c + d < C : c - d >= 0); ++d) {
-      const T l = lk[d];
-      if (l + X < fl) break;
-      const int k = c + sgnd * d;
-      const T ex = Op::ex((l - m) + row[k]);
-      sum += (!SIGNED || sgn[k]) ? ex : -ex;
-    }
-  }
-  const int dmax = d - 1;  // the last tap distance summed
-  *taps += 1 + min(dmax, c) + min(dmax, C - 1 - c);
+  if (d > dend) return false;
+  const T l = lk[d];
+  if (l + X < g.mtail) return false;
+  const int pl = c0 - d, pr = c0 + 3 + d;  // the two new taps (positions pl & 3 = -d & 3, pr & 3 = (3 + d) & 3)
+  constexpr int il = (4 - DM) & 3, ir = (3 + DM) & 3;
+  g.lq[il] = pl >= 0 ? row[pl] : Op::kNone;
+  g.rq[ir] = pr < C ? row[pr] : Op::kNone;
   if (SIGNED) {
-    *pos = sum >= T(0);
-    return (Op::lg(fabs(sum)) + m) * Op::kUnscale;
+    g.lsg[il] = (pl >= 0 && !sgn[pl]) ? T(-1) : T(1);
+    g.rsg[ir] = (pr < C && !sgn[pr]) ? T(-1) : T(1);
   }
-  *pos = true;
-  return (Op::lg(sum) + m) * Op::kUnscale;
+  T a[4], b[4];
+  bool up = false;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const T lm = l - g.m[j];
+    a[j] = g.lq[(j - DM) & 3] + lm;
+    b[j] = g.rq[(j + DM) & 3] + lm;
+    up |= a[j] > T(0) || b[j] > T(0);
+  }
+  if (up) {  // a new maximum for some output: shift its sum (t = 0 leaves an output unchanged)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      T t = a[j] > b[j] ? a[j] : b[j];
+      t = t > T(0) ? t : T(0);
+      g.s[j] *= Op::ex(-t);
+      g.m[j] += t;
+      a[j] -= t;
+      b[j] -= t;
+    }
+    log_group_mtail(g);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (SIGNED) {
+      g.s[j] += g.lsg[(j - DM) & 3] * Op::ex(a[j]);
+      g.s[j] += g.rsg[(j + DM) & 3] * Op::ex(b[j]);
+    } else {
+      g.s[j] += Op::ex(a[j]);
+      g.s[j] += Op::ex(b[j]);
+    }
+  }
+  return true;
+}
+
+// Outputs c0..c0+3 of one staged row (those below C are valid): v[j] and, when
+// SIGNED, pos[j] (sum >= 0).  Returns the exponentials evaluated per valid output.
+template <typename T, bool SIGNED>
+__device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_t* __restrict__ sgn,
+                                         const T* __restrict__ lk, T X, int c0, int C, T* v, bool* pos) {
+  using Op = LogOps<T>;
+  LogGroup<T> g;
+  g.nv = min(4, C - c0);
+  // row positions c0-1 .. c0+4, taps outside the row as kNone
+  T x[6], sx[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const int p = c0 - 1 + i;
+    const bool in = p >= 0 && p < C;
+    x[i] = in ? row[p] : Op::kNone;
+    sx[i] = (SIGNED && in && !sgn[p]) ? T(-1) : T(1);
+  }
+  // distances 0 and 1: m = max(centre, neighbours + lk[1], floor)
+  const T l1 = C > 1 ? lk[1] : Op::kNone;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const T cx = x[j + 1], lx = x[j], rx = x[j + 2];
+    const T nb = (lx > rx ? lx : rx) + l1;
+    T m = cx > Op::kFloor ? cx : Op::kFloor;
+    m = nb > m ? nb : m;
+    const T lm = l1 - m;
+    T s = SIGNED ? sx[j + 1] * Op::ex(cx - m) : Op::ex(cx - m);
+    if (SIGNED) {
+      s += sx[j] * Op::ex(lx + lm);
+      s += sx[j + 2] * Op::ex(rx + lm);
+    } else {
+      s += Op::ex(lx + lm);
+      s += Op::ex(rx + lm);
+    }
+    g.m[j] = m;
+    g.s[j] = s;
+  }
+  // rings for distance 1 (left taps at c0-1..c0+2, right taps at c0+1..c0+4)
+  g.lq[0] = x[1]; g.lq[1] = x[2]; g.lq[2] = x[3]; g.lq[3] = x[0];
+  g.rq[0] = x[5]; g.rq[1] = x[2]; g.rq[2] = x[3]; g.rq[3] = x[4];
+  if (SIGNED) {
+    g.lsg[0] = sx[1]; g.lsg[1] = sx[2]; g.lsg[2] = sx[3]; g.lsg[3] = sx[0];
+    g.rsg[0] = sx[5]; g.rsg[1] = sx[2]; g.rsg[2] = sx[3]; g.rsg[3] = sx[4];
+  }
+  log_group_mtail(g);
+  // beyond dend every tap of every valid output lies outside the row
+  const int dend = max(min(c0 + 3, C - 1), C - 1 - c0);
+  int d = 2;
+  for (;;) {
+    if (!log_group_step<T, SIGNED, 2>(g, row, sgn, lk, X, c0, C, d, dend)) break;
+    ++d;
+    if (!log_group_step<T, SIGNED, 3>(g, row, sgn, lk, X, c0, C, d, dend)) break;
+    ++d;
+    if (!log_group_step<T, SIGNED, 0>(g, row, sgn, lk, X, c0, C, d, dend)) break;
+    ++d;
+    if (!log_group_step<T, SIGNED, 1>(g, row, sgn, lk, X, c0, C, d, dend)) break;
+    ++d;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (SIGNED) {
+      pos[j] = g.s[j] >= T(0);
+      v[j] = (Op::lg(fabs(g.s[j])) + g.m[j]) * Op::kUnscale;
+    } else {
+      pos[j] = true;
+      v[j] = (Op::lg(g.s[j]) + g.m[j]) * Op::kUnscale;
+    }
+  }
+  return 3 + 2 * (d - 2);
 }
 
 // Stage LR rows of one image in SMEM (odd row stride CP), their signs, the row
-// maxima X and the tap table lk[d] = -d^2/gamma (scaled).
+// maxima X and the tap table lk[d] = -d^2/gamma (scaled).  Rows whose length
+// and start allow it are read as 16-byte vectors.
 template <typename T, bool SIGNED, int LR>
 __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_t* __restrict__ in_sign,
                                           T* rows, uint8_t* sg, T* xmax, T* lk, size_t base, int r0, int nr,
                                           int C, int CP, int SP, T gamma_t) {
   using Op = LogOps<T>;
+  constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool vec = (C % V) == 0 && (base % V) == 0 && ((uintptr_t)in & 15) == 0;
   // warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
   for (int rr = warp; rr < LR; rr += 8) {
     T vm = Op::kFloor;
-    for (int k = lane; k < C; k += 32) {
-      T v = Op::kFloor;
-      uint8_t sv = 1;
-      if (rr < nr) {
-        v = in[base + (size_t)(r0 + rr) * C + k] * Op::kScale;
-        if (SIGNED) sv = in_sign[base + (size_t)(r0 + rr) * C + k];
+    const size_t ro = base + (size_t)(r0 + rr) * C;
+    if (vec && rr < nr) {
+      for (int k = lane * V; k < C; k += 32 * V) {
+        T t[V];
+        if constexpr (V == 4) {
+          const float4 f = *reinterpret_cast<const float4*>(in + ro + k);
+          t[0] = f.x; t[1] = f.y; t[2] = f.z; t[3] = f.w;
+        } else {
+          const double2 f = *reinterpret_cast<const double2*>(in + ro + k);
+          t[0] = f.x; t[1] = f.y;
+        }
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          const T v = t[i] * Op::kScale;
+          rows[rr * CP + k + i] = v;
+          if (SIGNED) sg[rr * SP + k + i] = in_sign[ro + k + i];
+          vm = v > vm ? v : vm;
+        }
       }
-      rows[rr * CP + k] = v;
-      if (SIGNED) sg[rr * SP + k] = sv;
-      vm = v > vm ? v : vm;
+    } else {
+      for (int k = lane; k < C; k += 32) {
+        T v = Op::kFloor;
+        uint8_t sv = 1;
+        if (rr < nr) {
+          v = in[ro + k] * Op::kScale;
+          if (SIGNED) sv = in_sign[ro + k];
+        }
+        rows[rr * CP + k] = v;
+        if (SIGNED) sg[rr * SP + k] = sv;
+        vm = v > vm ? v : vm;
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -254,9 +373,9 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
   for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d) * T(d) / gamma_t * Op::kScale;
 }
 
-// Layout "rows fastest": a block owns LR rows of one image and thread e makes
-// output (c = e / LR, rr = e % LR), so the stores out[c][r0 + rr] of a warp are
-// contiguous runs.
+// Thread e makes group (c0 = 4 (e / LR), row rr = e % LR): the 32 lanes of a
+// warp read 32 rows' taps at one position (conflict-free with the odd stride
+// when LR = 32) and store runs out[c][r0 + rr] of consecutive rows.
 template <typename T, bool SIGNED, int LR>
 __global__ void __launch_bounds__(256) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
@@ -275,68 +394,25 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
   const int lane = threadIdx.x & 31;
   log_stage<T, SIGNED, LR>(in, in_sign, rows, sg, xmax, lk, base, r0, nr, C, CP, SP, gamma_t);
   __syncthreads();
+  const int G = (C + 3) >> 2;
   unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
-  for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
-    const int c = e / LR, rr = e - c * LR;
+  for (int e = threadIdx.x; e < LR * G; e += blockDim.x) {
+    const int gi = e / LR, rr = e - gi * LR;
     if (rr >= nr) continue;
-    bool pos;
-    const T v = log_out<T, SIGNED>(rows + rr * CP, sg + rr * SP, lk, xmax[rr], c, C, &pos, &n_ex);
-    const size_t o = base + (size_t)c * R + (r0 + rr);
-    out[o] = v;
-    if (SIGNED) out_sign[o] = pos ? 1 : 0;
-  }
-  if (exps) {
-    unsigned long long v = n_ex;
+    const int c0 = 4 * gi;
+    T v[4];
+    bool pos[4];
+    const int per = log_group<T, SIGNED>(rows + rr * CP, sg + rr * SP, lk, xmax[rr], c0, C, v, pos);
+    const int nv = min(4, C - c0);
+    n_ex += (unsigned)(per * nv);
+    const size_t o = base + (size_t)c0 * R + (r0 + rr);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) atomicAdd(exps, v);
-  }
-}
-
-// Layout "row per warp": warp w makes the outputs of rows w, w + 8, ..., its
-// lanes taking 32 consecutive c of one row, so the lanes of a warp run nearly
-// the same number of taps (neighbouring outputs of one row) and read
-// consecutive SMEM words; the results go through SMEM ([C][LR + 1]) and are
-// stored as contiguous runs of out[c][r0..].  Same outputs, bit for bit, as
-// the layout above.
-template <typename T, bool SIGNED, int LR>
-__global__ void __launch_bounds__(256) log_axis_pass_rowwarp_kernel(
-    const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
-    const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
-    unsigned long long* __restrict__ exps) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int CP = C + 1;
-  T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
-  T* lk = rows + LR * CP;                               // [C]
-  T* xmax = lk + C;                                     // [LR]
-  T* ot = xmax + LR;                                    // [C][LR + 1] results
-  uint8_t* sg = reinterpret_cast<uint8_t*>(ot + (size_t)C * (LR + 1));  // [LR][C + 4]
-  const int SP = C + 4;
-  uint8_t* osg = sg + LR * SP;                          // [C][LR + 1] result signs
-  const int r0 = blockIdx.x * LR;
-  const size_t base = (size_t)blockIdx.y * img_stride;
-  const int nr = min(LR, R - r0);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  log_stage<T, SIGNED, LR>(in, in_sign, rows, sg, xmax, lk, base, r0, nr, C, CP, SP, gamma_t);
-  __syncthreads();
-  unsigned n_ex = 0;
-  for (int rr = warp; rr < nr; rr += 8) {
-    const T* row = rows + rr * CP;
-    const uint8_t* sgn = sg + rr * SP;
-    const T X = xmax[rr];
-    for (int c = lane; c < C; c += 32) {
-      bool pos;
-      ot[(size_t)c * (LR + 1) + rr] = log_out<T, SIGNED>(row, sgn, lk, X, c, C, &pos, &n_ex);
-      if (SIGNED) osg[(size_t)c * (LR + 1) + rr] = pos ? 1 : 0;
+    for (int j = 0; j < 4; ++j) {
+      if (j < nv) {
+        out[o + (size_t)j * R] = v[j];
+        if (SIGNED) out_sign[o + (size_t)j * R] = pos[j] ? 1 : 0;
+      }
     }
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < LR * C; e += blockDim.x) {
-    const int c = e / LR, rr = e - c * LR;
-    if (rr >= nr) continue;
-    const size_t o = base + (size_t)c * R + (r0 + rr);
-    out[o] = ot[(size_t)c * (LR + 1) + rr];
-    if (SIGNED) out_sign[o] = osg[(size_t)c * (LR + 1) + rr];
   }
   if (exps) {
     unsigned long long v = n_ex;
@@ -347,16 +423,14 @@ __global__ void __launch_bounds__(256) log_axis_pass_rowwarp_kernel(
 }
 
 template <typename T>
-size_t log_axis_smem(int LR, int C, bool rowwarp = false) {
-  size_t b = ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
-  if (rowwarp) b += (size_t)C * (LR + 1) * (sizeof(T) + 1);
-  return b;
+size_t log_axis_smem(int LR, int C) {
+  return ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
 }
 
-template <typename T, int LR, bool ROWWARP>
+template <typename T, int LR>
 int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
                     const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
-  const size_t smem = log_axis_smem<T>(LR, C, ROWWARP);
+  const size_t smem = log_axis_smem<T>(LR, C);
   const T gamma_t = T(ctx->gamma);
   size_t done = 0;
   while (done < nimg) {
@@ -365,12 +439,12 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
     dim3 grid((R + LR - 1) / LR, (unsigned)chunk);
     size_t off = done * img_stride;
     if (in_sign) {
-      auto k = ROWWARP ? log_axis_pass_rowwarp_kernel<T, true, LR> : log_axis_pass_kernel<T, true, LR>;
+      auto k = log_axis_pass_kernel<T, true, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
                                 out_sign + off, ctx->profiling ? ctx->d_taps : nullptr);
     } else {
-      auto k = ROWWARP ? log_axis_pass_rowwarp_kernel<T, false, LR> : log_axis_pass_kernel<T, false, LR>;
+      auto k = log_axis_pass_kernel<T, false, LR>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr,
                                 ctx->profiling ? ctx->d_taps : nullptr);
@@ -381,18 +455,14 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
   return WDL_OK;
 }
 
-
 template <typename T>
 int log_axis_dispatch(wdl_ctx* ctx, int LR, const T* in, T* out, int R, int C, size_t nimg,
                       size_t img_stride, const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
-  // choice: rows per block (LR), plus 100 for the row-per-warp layout
+  // choice: rows per block
   switch (LR) {
-    case 8: return log_axis_launch<T, 8, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 32: return log_axis_launch<T, 32, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 108: return log_axis_launch<T, 8, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 116: return log_axis_launch<T, 16, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 132: return log_axis_launch<T, 32, true>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    default: return log_axis_launch<T, 16, false>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 8: return log_axis_launch<T, 8>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 16: return log_axis_launch<T, 16>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    default: return log_axis_launch<T, 32>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
   }
 }
 
@@ -412,7 +482,7 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
   cudaStreamIsCapturing(s, &cap);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
     return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-  const int cand[6] = {8, 16, 32, 108, 116, 132};
+  const int cand[3] = {8, 16, 32};
   int best = kLogRowsDefault;
   float best_ms = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -420,7 +490,7 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
   WDL_CUDA_TRY(ctx, cudaEventCreate(&e1));
   int rc = WDL_OK;
   for (int c : cand) {
-    if (log_axis_smem<T>(c % 100, C, c >= 100) > 200 * 1024) continue;
+    if (log_axis_smem<T>(c, C) > 200 * 1024) continue;
     // an untimed run first: the first launch of a variant also loads it
     if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s))) break;
     cudaEventRecord(e0, s);
