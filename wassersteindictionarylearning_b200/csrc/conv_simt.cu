@@ -173,6 +173,11 @@ struct LogOps<double> {
   __device__ static double lg(double x) { return log(x); }
 };
 
+// Rows are staged with kHalo taps of kNone on each side, so the loads of a
+// group need no range test while d <= c0 + kHalo on the left and
+// c0 + 3 + d < C + kHalo on the right.
+constexpr int kHalo = 8;
+
 // The state of one group of four outputs: running maxima m[j] and sums s[j],
 // and the taps of the current step in two 4-entry rings indexed by row
 // position mod 4 (left taps in lq, right taps in rq; their signs as +-1 in lsg
@@ -182,56 +187,74 @@ struct LogGroup {
   T m[4], s[4];
   T lq[4], rq[4];
   T lsg[4], rsg[4];
-  T mtail;  // min over the group's outputs of m - kTail
-  int nv;   // outputs of the group inside the row
+  T mmin;   // min over the group's outputs of m
+  T mtail;  // mmin - kTail
 };
 
-template <typename T>
-__device__ __forceinline__ void log_group_mtail(LogGroup<T>& g) {
+template <typename T, bool FULL>
+__device__ __forceinline__ void log_group_mmin(LogGroup<T>& g, int nv) {
   T mn = g.m[0];
 #pragma unroll
   for (int j = 1; j < 4; ++j)
-    if (j < g.nv) mn = g.m[j] < mn ? g.m[j] : mn;
+    if (FULL || j < nv) mn = g.m[j] < mn ? g.m[j] : mn;
+  g.mmin = mn;
   g.mtail = mn - LogOps<T>::kTail;
 }
 
-// One step at distance d (d & 3 == DM, d >= 2); false once the group is done.
-template <typename T, bool SIGNED, int DM>
+// One step at distance d (d & 3 == DM, d >= 2, d within the range the caller
+// checked); false once every output of the group has its sum.  GUARD: the two
+// new taps may lie beyond the halo.
+template <typename T, bool SIGNED, bool FULL, bool GUARD, int DM>
 __device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restrict__ row,
                                                const uint8_t* __restrict__ sgn, const T* __restrict__ lk,
-                                               T X, int c0, int C, int d, int dend) {
+                                               T X, int c0, int C, int d, int nv) {
   using Op = LogOps<T>;
-  if (d > dend) return false;
   const T l = lk[d];
-  if (l + X < g.mtail) return false;
-  const int pl = c0 - d, pr = c0 + 3 + d;  // the two new taps (positions pl & 3 = -d & 3, pr & 3 = (3 + d) & 3)
+  const T bound = l + X;  // no tap at distance >= d has a larger exponent
+  if (bound < g.mtail) return false;
+  const int pl = c0 - d, pr = c0 + 3 + d;  // the two new taps: pl & 3 = -d & 3, pr & 3 = (3 + d) & 3
   constexpr int il = (4 - DM) & 3, ir = (3 + DM) & 3;
-  g.lq[il] = pl >= 0 ? row[pl] : Op::kNone;
-  g.rq[ir] = pr < C ? row[pr] : Op::kNone;
-  if (SIGNED) {
-    g.lsg[il] = (pl >= 0 && !sgn[pl]) ? T(-1) : T(1);
-    g.rsg[ir] = (pr < C && !sgn[pr]) ? T(-1) : T(1);
+  if (GUARD) {
+    g.lq[il] = pl >= 0 ? row[pl] : Op::kNone;
+    g.rq[ir] = pr < C ? row[pr] : Op::kNone;
+    if (SIGNED) {
+      g.lsg[il] = (pl >= 0 && !sgn[pl]) ? T(-1) : T(1);
+      g.rsg[ir] = (pr < C && !sgn[pr]) ? T(-1) : T(1);
+    }
+  } else {
+    g.lq[il] = row[pl];
+    g.rq[ir] = row[pr];
+    if (SIGNED) {
+      g.lsg[il] = sgn[pl] ? T(1) : T(-1);
+      g.rsg[ir] = sgn[pr] ? T(1) : T(-1);
+    }
   }
   T a[4], b[4];
-  bool up = false;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const T lm = l - g.m[j];
     a[j] = g.lq[(j - DM) & 3] + lm;
     b[j] = g.rq[(j + DM) & 3] + lm;
-    up |= a[j] > T(0) || b[j] > T(0);
   }
-  if (up) {  // a new maximum for some output: shift its sum (t = 0 leaves an output unchanged)
+  // A new maximum is possible only while the bound exceeds some output's
+  // maximum; then shift the sums of the outputs that found one (t = 0 leaves
+  // an output unchanged).
+  if (bound > g.mmin) {
+    bool up = false;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      T t = a[j] > b[j] ? a[j] : b[j];
-      t = t > T(0) ? t : T(0);
-      g.s[j] *= Op::ex(-t);
-      g.m[j] += t;
-      a[j] -= t;
-      b[j] -= t;
+    for (int j = 0; j < 4; ++j) up |= a[j] > T(0) || b[j] > T(0);
+    if (up) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        T t = a[j] > b[j] ? a[j] : b[j];
+        t = t > T(0) ? t : T(0);
+        g.s[j] *= Op::ex(-t);
+        g.m[j] += t;
+        a[j] -= t;
+        b[j] -= t;
+      }
+      log_group_mmin<T, FULL>(g, nv);
     }
-    log_group_mtail(g);
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -246,22 +269,21 @@ __device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restri
   return true;
 }
 
-// Outputs c0..c0+3 of one staged row (those below C are valid): v[j] and, when
-// SIGNED, pos[j] (sum >= 0).  Returns the exponentials evaluated per valid output.
-template <typename T, bool SIGNED>
+// Outputs c0..c0+3 of one staged row (row[-kHalo..C+kHalo) readable; those
+// below C are valid; FULL: all four are): v[j] and, when SIGNED, pos[j]
+// (sum >= 0).  Returns the exponentials evaluated per output.
+template <typename T, bool SIGNED, bool FULL>
 __device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_t* __restrict__ sgn,
                                          const T* __restrict__ lk, T X, int c0, int C, T* v, bool* pos) {
   using Op = LogOps<T>;
   LogGroup<T> g;
-  g.nv = min(4, C - c0);
-  // row positions c0-1 .. c0+4, taps outside the row as kNone
+  const int nv = FULL ? 4 : min(4, C - c0);
+  // row positions c0-1 .. c0+4 (inside the halo: kNone beyond the row)
   T x[6], sx[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
-    const int p = c0 - 1 + i;
-    const bool in = p >= 0 && p < C;
-    x[i] = in ? row[p] : Op::kNone;
-    sx[i] = (SIGNED && in && !sgn[p]) ? T(-1) : T(1);
+    x[i] = row[c0 - 1 + i];
+    sx[i] = (SIGNED && !sgn[c0 - 1 + i]) ? T(-1) : T(1);
   }
   // distances 0 and 1: m = max(centre, neighbours + lk[1], floor)
   const T l1 = C > 1 ? lk[1] : Op::kNone;
@@ -290,19 +312,34 @@ __device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_
     g.lsg[0] = sx[1]; g.lsg[1] = sx[2]; g.lsg[2] = sx[3]; g.lsg[3] = sx[0];
     g.rsg[0] = sx[5]; g.rsg[1] = sx[2]; g.rsg[2] = sx[3]; g.rsg[3] = sx[4];
   }
-  log_group_mtail(g);
-  // beyond dend every tap of every valid output lies outside the row
+  log_group_mmin<T, FULL>(g, nv);
+  // beyond dend every tap of every valid output lies outside the row; up to
+  // dsafe both new taps of a step lie inside the halo
   const int dend = max(min(c0 + 3, C - 1), C - 1 - c0);
+  const int dsafe = min(dend, min(c0 + kHalo, C + kHalo - 4 - c0));
   int d = 2;
+  bool done = false;
   for (;;) {
-    if (!log_group_step<T, SIGNED, 2>(g, row, sgn, lk, X, c0, C, d, dend)) break;
+    if (d > dsafe) break;
+    if (!log_group_step<T, SIGNED, FULL, false, 2>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
+    if (++d > dsafe) break;
+    if (!log_group_step<T, SIGNED, FULL, false, 3>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
+    if (++d > dsafe) break;
+    if (!log_group_step<T, SIGNED, FULL, false, 0>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
+    if (++d > dsafe) break;
+    if (!log_group_step<T, SIGNED, FULL, false, 1>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
     ++d;
-    if (!log_group_step<T, SIGNED, 3>(g, row, sgn, lk, X, c0, C, d, dend)) break;
-    ++d;
-    if (!log_group_step<T, SIGNED, 0>(g, row, sgn, lk, X, c0, C, d, dend)) break;
-    ++d;
-    if (!log_group_step<T, SIGNED, 1>(g, row, sgn, lk, X, c0, C, d, dend)) break;
-    ++d;
+  }
+  // taps beyond the halo (groups near the row's ends with long reach)
+  for (; !done && d <= dend; ++d) {
+    bool go;
+    switch (d & 3) {
+      case 0: go = log_group_step<T, SIGNED, FULL, true, 0>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      case 1: go = log_group_step<T, SIGNED, FULL, true, 1>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      case 2: go = log_group_step<T, SIGNED, FULL, true, 2>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      default: go = log_group_step<T, SIGNED, FULL, true, 3>(g, row, sgn, lk, X, c0, C, d, nv); break;
+    }
+    if (!go) break;
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -317,9 +354,10 @@ __device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_
   return 3 + 2 * (d - 2);
 }
 
-// Stage LR rows of one image in SMEM (odd row stride CP), their signs, the row
-// maxima X and the tap table lk[d] = -d^2/gamma (scaled).  Rows whose length
-// and start allow it are read as 16-byte vectors.
+// Stage LR rows of one image in SMEM (row stride CP, odd, with kHalo taps of
+// kNone on each side), their signs (halo signs positive), the row maxima X and
+// the tap table lk[d] = -d^2/gamma (scaled).  Rows whose length and start
+// allow it are read as 16-byte vectors.
 template <typename T, bool SIGNED, int LR>
 __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_t* __restrict__ in_sign,
                                           T* rows, uint8_t* sg, T* xmax, T* lk, size_t base, int r0, int nr,
@@ -330,6 +368,16 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
   const bool vec = (C % V) == 0 && (base % V) == 0 && ((uintptr_t)in & 15) == 0;
   // warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
   for (int rr = warp; rr < LR; rr += 8) {
+    T* rw = rows + rr * CP + kHalo;
+    uint8_t* sw = sg + rr * SP + kHalo;
+    for (int k = lane; k < kHalo; k += 32) {
+      rw[-kHalo + k] = Op::kNone;
+      rw[C + k] = Op::kNone;
+      if (SIGNED) {
+        sw[-kHalo + k] = 1;
+        sw[C + k] = 1;
+      }
+    }
     T vm = Op::kFloor;
     const size_t ro = base + (size_t)(r0 + rr) * C;
     if (vec && rr < nr) {
@@ -345,8 +393,8 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           const T v = t[i] * Op::kScale;
-          rows[rr * CP + k + i] = v;
-          if (SIGNED) sg[rr * SP + k + i] = in_sign[ro + k + i];
+          rw[k + i] = v;
+          if (SIGNED) sw[k + i] = in_sign[ro + k + i];
           vm = v > vm ? v : vm;
         }
       }
@@ -358,8 +406,8 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
           v = in[ro + k] * Op::kScale;
           if (SIGNED) sv = in_sign[ro + k];
         }
-        rows[rr * CP + k] = v;
-        if (SIGNED) sg[rr * SP + k] = sv;
+        rw[k] = v;
+        if (SIGNED) sw[k] = sv;
         vm = v > vm ? v : vm;
       }
     }
@@ -373,21 +421,24 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
   for (int d = threadIdx.x; d < C; d += blockDim.x) lk[d] = -T(d) * T(d) / gamma_t * Op::kScale;
 }
 
+// SMEM row strides: values C + 2 kHalo + 1 (odd), sign bytes C + 2 kHalo + 4.
+__host__ __device__ constexpr int log_cp(int C) { return C + 2 * kHalo + 1; }
+__host__ __device__ constexpr int log_sp(int C) { return C + 2 * kHalo + 4; }
+
 // Thread e makes group (c0 = 4 (e / LR), row rr = e % LR): the 32 lanes of a
 // warp read 32 rows' taps at one position (conflict-free with the odd stride
 // when LR = 32) and store runs out[c][r0 + rr] of consecutive rows.
 template <typename T, bool SIGNED, int LR>
-__global__ void __launch_bounds__(256) log_axis_pass_kernel(
+__global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
     unsigned long long* __restrict__ exps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int CP = C + 1;                                 // odd row stride (elements)
+  const int CP = log_cp(C), SP = log_sp(C);
   T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
   T* lk = rows + LR * CP;                               // [C]: -d^2/gamma (scaled)
   T* xmax = lk + C;                                     // [LR]
-  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);  // [LR][C + 4] (bank-spread bytes)
-  const int SP = C + 4;
+  uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);  // [LR][SP] (SIGNED)
   const int r0 = blockIdx.x * LR;
   const size_t base = (size_t)blockIdx.y * img_stride;
   const int nr = min(LR, R - r0);
@@ -395,22 +446,33 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
   log_stage<T, SIGNED, LR>(in, in_sign, rows, sg, xmax, lk, base, r0, nr, C, CP, SP, gamma_t);
   __syncthreads();
   const int G = (C + 3) >> 2;
+  const bool full = (C & 3) == 0;
   unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
   for (int e = threadIdx.x; e < LR * G; e += blockDim.x) {
     const int gi = e / LR, rr = e - gi * LR;
     if (rr >= nr) continue;
     const int c0 = 4 * gi;
+    const T* row = rows + rr * CP + kHalo;
+    const uint8_t* sgn = sg + rr * SP + kHalo;
     T v[4];
     bool pos[4];
-    const int per = log_group<T, SIGNED>(rows + rr * CP, sg + rr * SP, lk, xmax[rr], c0, C, v, pos);
-    const int nv = min(4, C - c0);
-    n_ex += (unsigned)(per * nv);
     const size_t o = base + (size_t)c0 * R + (r0 + rr);
+    if (full) {
+      n_ex += 4u * log_group<T, SIGNED, true>(row, sgn, lk, xmax[rr], c0, C, v, pos);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (j < nv) {
+      for (int j = 0; j < 4; ++j) {
         out[o + (size_t)j * R] = v[j];
         if (SIGNED) out_sign[o + (size_t)j * R] = pos[j] ? 1 : 0;
+      }
+    } else {
+      const int nv = min(4, C - c0);
+      n_ex += (unsigned)nv * log_group<T, SIGNED, false>(row, sgn, lk, xmax[rr], c0, C, v, pos);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (j < nv) {
+          out[o + (size_t)j * R] = v[j];
+          if (SIGNED) out_sign[o + (size_t)j * R] = pos[j] ? 1 : 0;
+        }
       }
     }
   }
@@ -424,7 +486,7 @@ __global__ void __launch_bounds__(256) log_axis_pass_kernel(
 
 template <typename T>
 size_t log_axis_smem(int LR, int C) {
-  return ((size_t)LR * (C + 1) + C + LR) * sizeof(T) + (size_t)LR * (C + 4) + 16;
+  return ((size_t)LR * log_cp(C) + C + LR) * sizeof(T) + (size_t)LR * log_sp(C) + 16;
 }
 
 template <typename T, int LR>

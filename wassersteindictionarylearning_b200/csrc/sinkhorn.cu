@@ -186,10 +186,15 @@ __global__ void k_poison_out_of_range(T* __restrict__ bary, const int* __restric
 }
 
 // ---------------- log-domain forward (:700-720, :167-196) ---------------------------
+// Thread per dictionary entry q, histograms p in order (no index division).
 template <typename T>
 __global__ void k_log_sub_atoms(const T* __restrict__ log_atoms, const T* __restrict__ cb,
-                                T* __restrict__ a, size_t KN, size_t total) {
-  GRID_STRIDE(i, total) a[i] = log_atoms[i % KN] - cb[i];
+                                T* __restrict__ a, size_t KN, int P) {
+  GRID_STRIDE(q, KN) {
+    const T lp = log_atoms[q];
+#pragma unroll 4
+    for (int p = 0; p < P; ++p) a[(size_t)p * KN + q] = lp - cb[(size_t)p * KN + q];
+  }
 }
 
 template <typename T>
@@ -393,17 +398,27 @@ __global__ void k_lbwd_pre(const T* __restrict__ n, const T* __restrict__ v,
   if (threadIdx.x == 0) part[pk * gridDim.y + blockIdx.y] = acc;
 }
 
+// Thread per dictionary entry q = (k, j), histograms p in order: the
+// dictionary gradient gdic[q] (KN doubles, summed over p here rather than kept
+// per histogram) takes this round's sum over p in one update.
 template <typename T>
 __global__ void k_lbwd_mid(const T* __restrict__ c, const T* __restrict__ cb,
                            const T* __restrict__ log_atoms, const uint8_t* __restrict__ sd,
-                           double* __restrict__ gdic, T* __restrict__ nxt, size_t KN, size_t PKN,
-                           int weights) {
-  GRID_STRIDE(i, PKN) {
-    const T cbv = cb[i], cc = c[i], lp = log_atoms[i % KN];
-    const T e = d_exp<T>(cc - cbv);
-    gdic[i] += (double)(sd[i] ? e : -e);
-    nxt[i] = lp + cc - T(2) * cbv;
-    if (weights) nxt[PKN + i] = c[PKN + i] + (lp - T(2) * cbv);
+                           double* __restrict__ gdic, T* __restrict__ nxt, size_t KN, int P,
+                           size_t PKN, int weights) {
+  GRID_STRIDE(q, KN) {
+    const T lp = log_atoms[q];
+    double g = 0;
+#pragma unroll 4
+    for (int p = 0; p < P; ++p) {
+      const size_t i = (size_t)p * KN + q;
+      const T cbv = cb[i], cc = c[i];
+      const T e = d_exp<T>(cc - cbv);
+      g += (double)(sd[i] ? e : -e);
+      nxt[i] = lp + cc - T(2) * cbv;
+      if (weights) nxt[PKN + i] = c[PKN + i] + (lp - T(2) * cbv);
+    }
+    gdic[q] += g;
   }
 }
 
@@ -430,6 +445,75 @@ __global__ void k_lbwd_post(const T* __restrict__ c2, const T* __restrict__ phi_
     n[idx] = sn;
     gw[idx] = sg;
   }
+}
+
+// Round s's k_lbwd_post followed by round s-1's k_lbwd_pre in one pass: the
+// post's v, r, n and gw feed only that pre, whose b and phi are the post's b_p
+// and phi_p, so v, r, n and gw never go to memory.  Block per (p, segment)
+// with one warp per atom (blockDim 32 K, K <= kFuseK): lane jj of warp k
+// handles pixels j0 + jj + 32 m of atom k, two 32-pixel chunks per round.
+// Each warp makes its atom's v and r, the block sums n and gw over the atoms
+// through SMEM (k in order, as k_lbwd_post), then each warp applies the pre to
+// its atom.  The dot partial of (p, k) over the segment is the lanes' sums
+// reduced across the warp, an order fixed by N alone.
+constexpr int kFuseK = 32;
+template <typename T>
+__global__ void __launch_bounds__(1024) k_lbwd_post_pre(
+    const T* __restrict__ c2, const T* __restrict__ phi_p, const T* __restrict__ b_p,
+    uint8_t* __restrict__ sd, uint8_t* __restrict__ sw, const T* __restrict__ lam,
+    T* __restrict__ tmp, T* __restrict__ u, double* __restrict__ part, int K, size_t N, size_t PKN) {
+  extern __shared__ __align__(16) unsigned char fuse_raw[];
+  T* vs = reinterpret_cast<T*>(fuse_raw);  // [K][64] v of this round's pixels
+  T* rs = vs + K * 64;                     // [K][64] r
+  const int k = threadIdx.x >> 5, jj = threadIdx.x & 31;
+  const size_t p = blockIdx.x;
+  const size_t j0 = (size_t)blockIdx.y * kSegElems, j1 = min(N, j0 + kSegElems);
+  const T l = lam[p * K + k];
+  const size_t ib = (p * K + k) * N;
+  double acc = 0;
+  for (size_t jb = j0; jb < j1; jb += 64) {
+    T vv[2], rr[2], ph[2], bp[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t j = jb + 32 * h + jj;
+      vv[h] = rr[h] = ph[h] = bp[h] = T(0);
+      if (j < j1) {
+        const size_t i = ib + j;
+        ph[h] = phi_p[i];
+        bp[h] = b_p[i];
+        T e = d_exp<T>(c2[i] - ph[h]);
+        vv[h] = sd[i] ? e : -e;
+        e = d_exp<T>(c2[PKN + i] + bp[h]);
+        rr[h] = sw[i] ? e : -e;
+      }
+      vs[k * 64 + 32 * h + jj] = vv[h];
+      rs[k * 64 + 32 * h + jj] = rr[h];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      T sn = T(0), sg = T(0);
+      for (int q = 0; q < K; ++q) {
+        sn -= vs[q * 64 + 32 * h + jj];
+        sg -= rs[q * 64 + 32 * h + jj];
+      }
+      const size_t j = jb + 32 * h + jj;
+      if (j < j1) {
+        const size_t i = ib + j;
+        const T x = l * sn + vv[h];
+        sd[i] = x >= T(0);
+        tmp[i] = d_log<T>(fabs(x)) + bp[h];
+        acc += (double)ph[h] * (double)sg;
+        const T y = l * sg + rr[h];
+        sw[i] = y >= T(0);
+        u[i] = d_log<T>(fabs(y)) - ph[h];
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (jj == 0) part[(p * K + k) * gridDim.y + blockIdx.y] = acc;
 }
 
 // ---------------- reductions and evaluate_both epilogue (:1086-1136) ----------------
@@ -646,7 +730,7 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       if ((rc = log_conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, nullptr, nullptr,
                                   nullptr, s)))
         return rc;
-      k_log_sub_atoms<T><<<G_PKN, 256, 0, s>>>(B.atoms, cb, B.a, KN, PKN);
+      k_log_sub_atoms<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.atoms, cb, B.a, KN, P);
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = log_conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, nullptr, nullptr,
                                   nullptr, s)))
@@ -676,7 +760,8 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
   const int dict = (result_dic || log_domain) ? 1 : 0;
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.v, 0, PKN * sizeof(T), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.r, 0, PKN * sizeof(T), s));
-  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, PKN * sizeof(double), s));
+  // the log domain sums the dictionary gradient over p as it goes (KN entries)
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, (log_domain ? KN : PKN) * sizeof(double), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.dot, 0, (size_t)P * K * sizeof(double), s));
   T* tmp = B.buf2;
   T* u = B.buf2 + PKN;
@@ -712,31 +797,41 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN, dict);
       WDL_LAUNCH_CHECK(ctx);
     } else {
-      k_lbwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
-          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.sd, B.sw, B.dpart, K, N);
-      WDL_LAUNCH_CHECK(ctx);
+      // the first round's pre here; later rounds' pre ran with the previous post
+      if (sstep == L || K > kFuseK) {
+        k_lbwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
+            B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.sd, B.sw, B.dpart, K, N);
+        WDL_LAUNCH_CHECK(ctx);
+      }
       k_add_partials<<<(P * K + 127) / 128, 128, 0, s>>>(B.dot, B.dpart, P * K, (int)n_segments(N));
       WDL_LAUNCH_CHECK(ctx);
       // sd and sw are adjacent, so the pair is one 2*P*K-image signed operand.
       if ((rc = log_conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, B.sd, B.sd, B.stmp, s)))
         return rc;
-      k_lbwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.sd, B.gdic, B.buf2, KN, PKN,
-                                          more);
+      k_lbwd_mid<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.sd, B.gdic, B.buf2,
+                                                        KN, P, PKN, more);
       WDL_LAUNCH_CHECK(ctx);
       if (!more) break;
       if ((rc = log_conv_stack<T>(ctx, B.buf2, B.cbuf2, B.ctmp, nimg, B.sd, B.sd, B.stmp, s)))
         return rc;
       const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
       const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
-      k_lbwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.sd, B.sw, B.v, B.r, B.n, B.gw,
-                                          K, N, PN, PKN);
+      if (K <= kFuseK) {
+        k_lbwd_post_pre<T><<<dim3((unsigned)P, (unsigned)n_segments(N)), 32 * K, 2 * K * 64 * sizeof(T), s>>>(
+            B.cbuf2, phi_p, b_p, B.sd, B.sw, B.lam, tmp, u, B.dpart, K, N, PKN);
+      } else {
+        k_lbwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.sd, B.sw, B.v, B.r, B.n, B.gw,
+                                            K, N, PN, PKN);
+      }
       WDL_LAUNCH_CHECK(ctx);
     }
   }
 
   // Outputs.
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
-  if (result_dic) {
+  if (result_dic && log_domain) {
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_dic, B.gdic, KN * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else if (result_dic) {
     k_sum_over_p<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
     WDL_LAUNCH_CHECK(ctx);
   }
@@ -798,7 +893,7 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
     } else {
       if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
         return rc;
-      k_log_sub_atoms<T><<<launch_cfg(ctx, PKN), 256, 0, s>>>(at, conv, a, KN, PKN);
+      k_log_sub_atoms<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(at, conv, a, KN, (int)(PKN / KN));
       WDL_LAUNCH_CHECK(ctx);
       if ((rc = log_conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
         return rc;
