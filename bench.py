@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd Sinkhorn iters/s (128², K=5) vs plain FP32; p50/p99 serve latency"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
 # fused split-BF16 kernel on batched128 (P=64, L=100), from one ncu capture.
-FUSED_DRAM_BYTES_P64_L100 = 28.75e9
+FUSED_DRAM_BYTES_P64_L100 = 29.82e9
 UNIT = "hist-iter/s"
 WORKLOADS = {
     "batched128": dict(name="batched128", P=64, W=128, H=128, K=5, L=100, gamma=1.0, loss=4,

@@ -178,6 +178,19 @@ struct LogOps<double> {
 // c0 + 3 + d < C + kHalo on the right.
 constexpr int kHalo = 8;
 
+// +1 for sign byte 1, -1 for sign byte 0 (sign bytes are 0 or 1 throughout):
+// one integer multiply-add on the bit pattern of -1.
+template <typename T>
+__device__ __forceinline__ T sign_of(uint8_t b);
+template <>
+__device__ __forceinline__ float sign_of<float>(uint8_t b) {
+  return __uint_as_float(0xBF800000u + (uint32_t)b * 0x80000000u);
+}
+template <>
+__device__ __forceinline__ double sign_of<double>(uint8_t b) {
+  return __longlong_as_double((long long)(0xBFF0000000000000ull + (unsigned long long)b * 0x8000000000000000ull));
+}
+
 // The state of one group of four outputs: running maxima m[j] and sums s[j],
 // and the taps of the current step in two 4-entry rings indexed by row
 // position mod 4 (left taps in lq, right taps in rq; their signs as +-1 in lsg
@@ -191,45 +204,31 @@ struct LogGroup {
   T mtail;  // mmin - kTail
 };
 
+template <typename T>
+__device__ __forceinline__ T vmax(T a, T b) { return fmax(a, b); }
+template <>
+__device__ __forceinline__ float vmax<float>(float a, float b) { return fmaxf(a, b); }
+template <typename T>
+__device__ __forceinline__ T vmin(T a, T b) { return fmin(a, b); }
+template <>
+__device__ __forceinline__ float vmin<float>(float a, float b) { return fminf(a, b); }
+
 template <typename T, bool FULL>
 __device__ __forceinline__ void log_group_mmin(LogGroup<T>& g, int nv) {
   T mn = g.m[0];
 #pragma unroll
   for (int j = 1; j < 4; ++j)
-    if (FULL || j < nv) mn = g.m[j] < mn ? g.m[j] : mn;
+    if (FULL || j < nv) mn = vmin(mn, g.m[j]);
   g.mmin = mn;
   g.mtail = mn - LogOps<T>::kTail;
 }
 
-// One step at distance d (d & 3 == DM, d >= 2, d within the range the caller
-// checked); false once every output of the group has its sum.  GUARD: the two
-// new taps may lie beyond the halo.
-template <typename T, bool SIGNED, bool FULL, bool GUARD, int DM>
-__device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restrict__ row,
-                                               const uint8_t* __restrict__ sgn, const T* __restrict__ lk,
-                                               T X, int c0, int C, int d, int nv) {
+// The terms of one step at distance d (d & 3 == DM) whose two new taps are in
+// the rings: l = lk[d], bound = l + X.
+template <typename T, bool SIGNED, bool FULL, int DM>
+__device__ __forceinline__ void log_group_terms(LogGroup<T>& g, T l, T bound, int nv) {
   using Op = LogOps<T>;
-  const T l = lk[d];
-  const T bound = l + X;  // no tap at distance >= d has a larger exponent
-  if (bound < g.mtail) return false;
-  const int pl = c0 - d, pr = c0 + 3 + d;  // the two new taps: pl & 3 = -d & 3, pr & 3 = (3 + d) & 3
-  constexpr int il = (4 - DM) & 3, ir = (3 + DM) & 3;
-  if (GUARD) {
-    g.lq[il] = pl >= 0 ? row[pl] : Op::kNone;
-    g.rq[ir] = pr < C ? row[pr] : Op::kNone;
-    if (SIGNED) {
-      g.lsg[il] = (pl >= 0 && !sgn[pl]) ? T(-1) : T(1);
-      g.rsg[ir] = (pr < C && !sgn[pr]) ? T(-1) : T(1);
-    }
-  } else {
-    g.lq[il] = row[pl];
-    g.rq[ir] = row[pr];
-    if (SIGNED) {
-      g.lsg[il] = sgn[pl] ? T(1) : T(-1);
-      g.rsg[ir] = sgn[pr] ? T(1) : T(-1);
-    }
-  }
-  T a[4], b[4];
+  T a[4], b[4], t[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const T lm = l - g.m[j];
@@ -242,16 +241,18 @@ __device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restri
   if (bound > g.mmin) {
     bool up = false;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) up |= a[j] > T(0) || b[j] > T(0);
+    for (int j = 0; j < 4; ++j) {
+      t[j] = vmax(a[j], b[j]);
+      up |= t[j] > T(0);
+    }
     if (up) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        T t = a[j] > b[j] ? a[j] : b[j];
-        t = t > T(0) ? t : T(0);
-        g.s[j] *= Op::ex(-t);
-        g.m[j] += t;
-        a[j] -= t;
-        b[j] -= t;
+        const T tj = vmax(t[j], T(0));
+        g.s[j] *= Op::ex(-tj);
+        g.m[j] += tj;
+        a[j] -= tj;
+        b[j] -= tj;
       }
       log_group_mmin<T, FULL>(g, nv);
     }
@@ -266,6 +267,48 @@ __device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* __restri
       g.s[j] += Op::ex(b[j]);
     }
   }
+}
+
+// Step d = d0 + K (d & 3 == DM) of a block of four inside the halo: the taps
+// come from lp[-K] and rp[K] (lp = row + c0 - d0, rp = row + c0 + 3 + d0) and
+// the weight from lkp[K] (lkp = lk + d0), immediate offsets from one base per
+// block.  False once every output of the group has its sum.
+template <typename T, bool SIGNED, bool FULL, int DM, int K>
+__device__ __forceinline__ bool log_group_step(LogGroup<T>& g, const T* lkp, const T* lp, const T* rp,
+                                               const uint8_t* lsp, const uint8_t* rsp, T X, int nv) {
+  const T l = lkp[K];
+  const T bound = l + X;  // no tap at distance >= d has a larger exponent
+  if (bound < g.mtail) return false;
+  constexpr int il = (4 - DM) & 3, ir = (3 + DM) & 3;  // ring slots of positions c0 - d, c0 + 3 + d
+  g.lq[il] = lp[-K];
+  g.rq[ir] = rp[K];
+  if (SIGNED) {
+    g.lsg[il] = sign_of<T>(lsp[-K]);
+    g.rsg[ir] = sign_of<T>(rsp[K]);
+  }
+  log_group_terms<T, SIGNED, FULL, DM>(g, l, bound, nv);
+  return true;
+}
+
+// Step d (d & 3 == DM) whose taps may lie beyond the halo.
+template <typename T, bool SIGNED, bool FULL, int DM>
+__device__ __forceinline__ bool log_group_step_guarded(LogGroup<T>& g, const T* __restrict__ row,
+                                                       const uint8_t* __restrict__ sgn,
+                                                       const T* __restrict__ lk, T X, int c0, int C, int d,
+                                                       int nv) {
+  using Op = LogOps<T>;
+  const T l = lk[d];
+  const T bound = l + X;
+  if (bound < g.mtail) return false;
+  const int pl = c0 - d, pr = c0 + 3 + d;
+  constexpr int il = (4 - DM) & 3, ir = (3 + DM) & 3;
+  g.lq[il] = pl >= 0 ? row[pl] : Op::kNone;
+  g.rq[ir] = pr < C ? row[pr] : Op::kNone;
+  if (SIGNED) {
+    g.lsg[il] = pl >= 0 ? sign_of<T>(sgn[pl]) : T(1);
+    g.rsg[ir] = pr < C ? sign_of<T>(sgn[pr]) : T(1);
+  }
+  log_group_terms<T, SIGNED, FULL, DM>(g, l, bound, nv);
   return true;
 }
 
@@ -283,16 +326,14 @@ __device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
     x[i] = row[c0 - 1 + i];
-    sx[i] = (SIGNED && !sgn[c0 - 1 + i]) ? T(-1) : T(1);
+    sx[i] = SIGNED ? sign_of<T>(sgn[c0 - 1 + i]) : T(1);
   }
   // distances 0 and 1: m = max(centre, neighbours + lk[1], floor)
   const T l1 = C > 1 ? lk[1] : Op::kNone;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const T cx = x[j + 1], lx = x[j], rx = x[j + 2];
-    const T nb = (lx > rx ? lx : rx) + l1;
-    T m = cx > Op::kFloor ? cx : Op::kFloor;
-    m = nb > m ? nb : m;
+    const T m = vmax(vmax(cx, Op::kFloor), vmax(lx, rx) + l1);
     const T lm = l1 - m;
     T s = SIGNED ? sx[j + 1] * Op::ex(cx - m) : Op::ex(cx - m);
     if (SIGNED) {
@@ -319,25 +360,27 @@ __device__ __forceinline__ int log_group(const T* __restrict__ row, const uint8_
   const int dsafe = min(dend, min(c0 + kHalo, C + kHalo - 4 - c0));
   int d = 2;
   bool done = false;
-  for (;;) {
-    if (d > dsafe) break;
-    if (!log_group_step<T, SIGNED, FULL, false, 2>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
-    if (++d > dsafe) break;
-    if (!log_group_step<T, SIGNED, FULL, false, 3>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
-    if (++d > dsafe) break;
-    if (!log_group_step<T, SIGNED, FULL, false, 0>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
-    if (++d > dsafe) break;
-    if (!log_group_step<T, SIGNED, FULL, false, 1>(g, row, sgn, lk, X, c0, C, d, nv)) { done = true; break; }
-    ++d;
+  // blocks of four steps inside the halo (d = 2 mod 4 at each block's start)
+  while (d + 3 <= dsafe) {
+    const T* lkp = lk + d;
+    const T* lp = row + (c0 - d);
+    const T* rp = row + (c0 + 3 + d);
+    const uint8_t* lsp = SIGNED ? sgn + (c0 - d) : nullptr;
+    const uint8_t* rsp = SIGNED ? sgn + (c0 + 3 + d) : nullptr;
+    if (!log_group_step<T, SIGNED, FULL, 2, 0>(g, lkp, lp, rp, lsp, rsp, X, nv)) { done = true; break; }
+    if (!log_group_step<T, SIGNED, FULL, 3, 1>(g, lkp, lp, rp, lsp, rsp, X, nv)) { done = true; d += 1; break; }
+    if (!log_group_step<T, SIGNED, FULL, 0, 2>(g, lkp, lp, rp, lsp, rsp, X, nv)) { done = true; d += 2; break; }
+    if (!log_group_step<T, SIGNED, FULL, 1, 3>(g, lkp, lp, rp, lsp, rsp, X, nv)) { done = true; d += 3; break; }
+    d += 4;
   }
-  // taps beyond the halo (groups near the row's ends with long reach)
+  // the remaining steps, with range tests
   for (; !done && d <= dend; ++d) {
     bool go;
     switch (d & 3) {
-      case 0: go = log_group_step<T, SIGNED, FULL, true, 0>(g, row, sgn, lk, X, c0, C, d, nv); break;
-      case 1: go = log_group_step<T, SIGNED, FULL, true, 1>(g, row, sgn, lk, X, c0, C, d, nv); break;
-      case 2: go = log_group_step<T, SIGNED, FULL, true, 2>(g, row, sgn, lk, X, c0, C, d, nv); break;
-      default: go = log_group_step<T, SIGNED, FULL, true, 3>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      case 0: go = log_group_step_guarded<T, SIGNED, FULL, 0>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      case 1: go = log_group_step_guarded<T, SIGNED, FULL, 1>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      case 2: go = log_group_step_guarded<T, SIGNED, FULL, 2>(g, row, sgn, lk, X, c0, C, d, nv); break;
+      default: go = log_group_step_guarded<T, SIGNED, FULL, 3>(g, row, sgn, lk, X, c0, C, d, nv); break;
     }
     if (!go) break;
   }
@@ -366,6 +409,8 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
   constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool vec = (C % V) == 0 && (base % V) == 0 && ((uintptr_t)in & 15) == 0;
+  // sign bytes four at a time (FP32 rows: SP and kHalo keep the SMEM rows 4-aligned)
+  const bool vsg = SIGNED && V == 4 && vec && ((uintptr_t)in_sign & 3) == 0;
   // warp w owns rows w, w + 8, ..., so the row maxima come from shuffles
   for (int rr = warp; rr < LR; rr += 8) {
     T* rw = rows + rr * CP + kHalo;
@@ -380,22 +425,25 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
     }
     T vm = Op::kFloor;
     const size_t ro = base + (size_t)(r0 + rr) * C;
+    const T* ir = in + ro;
+    const uint8_t* isr = SIGNED ? in_sign + ro : nullptr;
     if (vec && rr < nr) {
       for (int k = lane * V; k < C; k += 32 * V) {
         T t[V];
         if constexpr (V == 4) {
-          const float4 f = *reinterpret_cast<const float4*>(in + ro + k);
+          const float4 f = *reinterpret_cast<const float4*>(ir + k);
           t[0] = f.x; t[1] = f.y; t[2] = f.z; t[3] = f.w;
         } else {
-          const double2 f = *reinterpret_cast<const double2*>(in + ro + k);
+          const double2 f = *reinterpret_cast<const double2*>(ir + k);
           t[0] = f.x; t[1] = f.y;
         }
+        if (SIGNED && vsg) *reinterpret_cast<uint32_t*>(sw + k) = *reinterpret_cast<const uint32_t*>(isr + k);
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           const T v = t[i] * Op::kScale;
           rw[k + i] = v;
-          if (SIGNED) sw[k + i] = in_sign[ro + k + i];
-          vm = v > vm ? v : vm;
+          if (SIGNED && !vsg) sw[k + i] = isr[k + i];
+          vm = vmax(vm, v);
         }
       }
     } else {
@@ -403,18 +451,18 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
         T v = Op::kFloor;
         uint8_t sv = 1;
         if (rr < nr) {
-          v = in[ro + k] * Op::kScale;
-          if (SIGNED) sv = in_sign[ro + k];
+          v = ir[k] * Op::kScale;
+          if (SIGNED) sv = isr[k];
         }
         rw[k] = v;
         if (SIGNED) sw[k] = sv;
-        vm = v > vm ? v : vm;
+        vm = vmax(vm, v);
       }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const T w = __shfl_xor_sync(0xffffffffu, vm, o);
-      vm = w > vm ? w : vm;
+      vm = vmax(vm, w);
     }
     if (lane == 0) xmax[rr] = vm;
   }
@@ -425,9 +473,10 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
 __host__ __device__ constexpr int log_cp(int C) { return C + 2 * kHalo + 1; }
 __host__ __device__ constexpr int log_sp(int C) { return C + 2 * kHalo + 4; }
 
-// Thread e makes group (c0 = 4 (e / LR), row rr = e % LR): the 32 lanes of a
-// warp read 32 rows' taps at one position (conflict-free with the odd stride
-// when LR = 32) and store runs out[c][r0 + rr] of consecutive rows.
+// Thread t makes the groups (c0 = 4 (t / LR + i 256 / LR)) of row rr = t % LR:
+// the 32 lanes of a warp read 32 rows' taps at one position (conflict-free
+// with the odd stride when LR = 32) and store runs out[c][r0 + rr] of
+// consecutive rows.
 template <typename T, bool SIGNED, int LR>
 __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
@@ -447,31 +496,35 @@ __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
   __syncthreads();
   const int G = (C + 3) >> 2;
   const bool full = (C & 3) == 0;
+  T* outi = out + base;
+  uint8_t* osi = SIGNED ? out_sign + base : nullptr;
   unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
-  for (int e = threadIdx.x; e < LR * G; e += blockDim.x) {
-    const int gi = e / LR, rr = e - gi * LR;
-    if (rr >= nr) continue;
+  // blockDim is a multiple of LR, so a thread keeps one row: rr = tid % LR,
+  // groups tid / LR, tid / LR + 256 / LR, ...
+  const int rr = threadIdx.x % LR;
+  const T* row = rows + rr * CP + kHalo;
+  const uint8_t* sgn = sg + rr * SP + kHalo;
+  const T X = xmax[rr];
+  for (int gi = threadIdx.x / LR; gi < G && rr < nr; gi += 256 / LR) {
     const int c0 = 4 * gi;
-    const T* row = rows + rr * CP + kHalo;
-    const uint8_t* sgn = sg + rr * SP + kHalo;
     T v[4];
     bool pos[4];
-    const size_t o = base + (size_t)c0 * R + (r0 + rr);
+    const int o = c0 * R + r0 + rr;  // offset in the image (R * C < 2^31, checked at launch)
     if (full) {
-      n_ex += 4u * log_group<T, SIGNED, true>(row, sgn, lk, xmax[rr], c0, C, v, pos);
+      n_ex += 4u * log_group<T, SIGNED, true>(row, sgn, lk, X, c0, C, v, pos);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        out[o + (size_t)j * R] = v[j];
-        if (SIGNED) out_sign[o + (size_t)j * R] = pos[j] ? 1 : 0;
+        outi[o + j * R] = v[j];
+        if (SIGNED) osi[o + j * R] = pos[j] ? 1 : 0;
       }
     } else {
       const int nv = min(4, C - c0);
-      n_ex += (unsigned)nv * log_group<T, SIGNED, false>(row, sgn, lk, xmax[rr], c0, C, v, pos);
+      n_ex += (unsigned)nv * log_group<T, SIGNED, false>(row, sgn, lk, X, c0, C, v, pos);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         if (j < nv) {
-          out[o + (size_t)j * R] = v[j];
-          if (SIGNED) out_sign[o + (size_t)j * R] = pos[j] ? 1 : 0;
+          outi[o + j * R] = v[j];
+          if (SIGNED) osi[o + j * R] = pos[j] ? 1 : 0;
         }
       }
     }
@@ -493,6 +546,8 @@ template <typename T, int LR>
 int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
                     const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
   const size_t smem = log_axis_smem<T>(LR, C);
+  if ((size_t)R * C >= (size_t)1 << 31)
+    return set_error(ctx, WDL_ERR_UNSUPPORTED, "log-domain operator: image of 2^31 values or more");
   const T gamma_t = T(ctx->gamma);
   size_t done = 0;
   while (done < nimg) {

@@ -451,65 +451,102 @@ __global__ void k_lbwd_post(const T* __restrict__ c2, const T* __restrict__ phi_
 // post's v, r, n and gw feed only that pre, whose b and phi are the post's b_p
 // and phi_p, so v, r, n and gw never go to memory.  Block per (p, segment)
 // with one warp per atom (blockDim 32 K, K <= kFuseK): lane jj of warp k
-// handles pixels j0 + jj + 32 m of atom k, two 32-pixel chunks per round.
-// Each warp makes its atom's v and r, the block sums n and gw over the atoms
-// through SMEM (k in order, as k_lbwd_post), then each warp applies the pre to
-// its atom.  The dot partial of (p, k) over the segment is the lanes' sums
-// reduced across the warp, an order fixed by N alone.
-constexpr int kFuseK = 32;
+// handles pixels j0 + jj + 32 m of atom k, kFuseH 32-pixel chunks per round.
+// Each warp makes its atom's v and r into SMEM; the block's threads then sum n
+// and gw over the atoms, one pixel and quantity per thread (k in order, as
+// k_lbwd_post); each warp applies the pre to its atom.  The next round's loads
+// are issued before this round's sums and pre, so they overlap them.  The dot
+// partial of (p, k) over the segment is the lanes' sums reduced across the
+// warp, an order fixed by N.
+constexpr int kFuseK = 32, kFuseH = 2;
+template <typename T>
+size_t post_pre_smem(int K) { return (size_t)(2 * K + 2) * 32 * kFuseH * sizeof(T); }
+
+template <typename T>
+struct PostPreIn {  // one round's inputs of one thread
+  T cv[kFuseH], cr[kFuseH], ph[kFuseH], bp[kFuseH];
+  uint8_t sv[kFuseH], sr[kFuseH];
+};
+
+template <typename T>
+__device__ __forceinline__ void post_pre_load(PostPreIn<T>& in, const T* __restrict__ c2,
+                                              const T* __restrict__ phi_p, const T* __restrict__ b_p,
+                                              const uint8_t* sd, const uint8_t* sw, size_t ib, size_t jb,
+                                              size_t j1, int jj, size_t PKN) {
+#pragma unroll
+  for (int h = 0; h < kFuseH; ++h) {
+    const size_t j = jb + 32 * h + jj;
+    in.cv[h] = in.cr[h] = in.ph[h] = in.bp[h] = T(0);
+    in.sv[h] = in.sr[h] = 1;
+    if (j < j1) {
+      const size_t i = ib + j;
+      in.cv[h] = c2[i];
+      in.cr[h] = c2[PKN + i];
+      in.ph[h] = phi_p[i];
+      in.bp[h] = b_p[i];
+      in.sv[h] = sd[i];
+      in.sr[h] = sw[i];
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(1024) k_lbwd_post_pre(
     const T* __restrict__ c2, const T* __restrict__ phi_p, const T* __restrict__ b_p,
     uint8_t* __restrict__ sd, uint8_t* __restrict__ sw, const T* __restrict__ lam,
     T* __restrict__ tmp, T* __restrict__ u, double* __restrict__ part, int K, size_t N, size_t PKN) {
+  constexpr int W = 32 * kFuseH;  // pixels per round
   extern __shared__ __align__(16) unsigned char fuse_raw[];
-  T* vs = reinterpret_cast<T*>(fuse_raw);  // [K][64] v of this round's pixels
-  T* rs = vs + K * 64;                     // [K][64] r
+  T* vs = reinterpret_cast<T*>(fuse_raw);  // [K][W] v of this round's pixels
+  T* rs = vs + K * W;                      // [K][W] r
+  T* sums = rs + K * W;                    // [2][W]: n, gw
   const int k = threadIdx.x >> 5, jj = threadIdx.x & 31;
   const size_t p = blockIdx.x;
   const size_t j0 = (size_t)blockIdx.y * kSegElems, j1 = min(N, j0 + kSegElems);
   const T l = lam[p * K + k];
   const size_t ib = (p * K + k) * N;
   double acc = 0;
-  for (size_t jb = j0; jb < j1; jb += 64) {
-    T vv[2], rr[2], ph[2], bp[2];
+  PostPreIn<T> cur, nxt;
+  post_pre_load(cur, c2, phi_p, b_p, sd, sw, ib, j0, j1, jj, PKN);
+  for (size_t jb = j0; jb < j1; jb += W) {
+    T vv[kFuseH], rr[kFuseH];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const size_t j = jb + 32 * h + jj;
-      vv[h] = rr[h] = ph[h] = bp[h] = T(0);
-      if (j < j1) {
-        const size_t i = ib + j;
-        ph[h] = phi_p[i];
-        bp[h] = b_p[i];
-        T e = d_exp<T>(c2[i] - ph[h]);
-        vv[h] = sd[i] ? e : -e;
-        e = d_exp<T>(c2[PKN + i] + bp[h]);
-        rr[h] = sw[i] ? e : -e;
-      }
-      vs[k * 64 + 32 * h + jj] = vv[h];
-      rs[k * 64 + 32 * h + jj] = rr[h];
+    for (int h = 0; h < kFuseH; ++h) {
+      T e = d_exp<T>(cur.cv[h] - cur.ph[h]);
+      vv[h] = cur.sv[h] ? e : -e;
+      e = d_exp<T>(cur.cr[h] + cur.bp[h]);
+      rr[h] = cur.sr[h] ? e : -e;
+      if (jb + 32 * h + jj >= j1) vv[h] = rr[h] = T(0);
+      vs[k * W + 32 * h + jj] = vv[h];
+      rs[k * W + 32 * h + jj] = rr[h];
+    }
+    __syncthreads();
+    // the next round's inputs (the elements this thread rewrites below are this round's)
+    if (jb + W < j1) post_pre_load(nxt, c2, phi_p, b_p, sd, sw, ib, jb + W, j1, jj, PKN);
+    for (int q = threadIdx.x; q < 2 * W; q += blockDim.x) {
+      const T* src = q < W ? vs + q : rs + (q - W);
+      T a = T(0);
+      for (int kk = 0; kk < K; ++kk) a -= src[kk * W];
+      sums[q] = a;
     }
     __syncthreads();
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      T sn = T(0), sg = T(0);
-      for (int q = 0; q < K; ++q) {
-        sn -= vs[q * 64 + 32 * h + jj];
-        sg -= rs[q * 64 + 32 * h + jj];
-      }
+    for (int h = 0; h < kFuseH; ++h) {
       const size_t j = jb + 32 * h + jj;
       if (j < j1) {
+        const T sn = sums[32 * h + jj], sg = sums[W + 32 * h + jj];
         const size_t i = ib + j;
         const T x = l * sn + vv[h];
         sd[i] = x >= T(0);
-        tmp[i] = d_log<T>(fabs(x)) + bp[h];
-        acc += (double)ph[h] * (double)sg;
+        tmp[i] = d_log<T>(fabs(x)) + cur.bp[h];
+        acc += (double)cur.ph[h] * (double)sg;
         const T y = l * sg + rr[h];
         sw[i] = y >= T(0);
-        u[i] = d_log<T>(fabs(y)) - ph[h];
+        u[i] = d_log<T>(fabs(y)) - cur.ph[h];
       }
     }
     __syncthreads();
+    cur = nxt;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -817,7 +854,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
       const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
       if (K <= kFuseK) {
-        k_lbwd_post_pre<T><<<dim3((unsigned)P, (unsigned)n_segments(N)), 32 * K, 2 * K * 64 * sizeof(T), s>>>(
+        const size_t smem = post_pre_smem<T>(K);
+        if (smem > 48 * 1024)
+          cudaFuncSetAttribute(k_lbwd_post_pre<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_lbwd_post_pre<T><<<dim3((unsigned)P, (unsigned)n_segments(N)), 32 * K, smem, s>>>(
             B.cbuf2, phi_p, b_p, B.sd, B.sw, B.lam, tmp, u, B.dpart, K, N, PKN);
       } else {
         k_lbwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.sd, B.sw, B.v, B.r, B.n, B.gw,
