@@ -477,11 +477,14 @@ __host__ __device__ constexpr int log_sp(int C) { return C + 2 * kHalo + 4; }
 // the 32 lanes of a warp read 32 rows' taps at one position (conflict-free
 // with the odd stride when LR = 32) and store runs out[c][r0 + rr] of
 // consecutive rows.
-template <typename T, bool SIGNED, int LR>
+// SUB: also write sub_out = sub_from (period sub_k images) - out, image by
+// image (img0: the launch's first image).
+template <typename T, bool SIGNED, int LR, bool SUB>
 __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
-    unsigned long long* __restrict__ exps) {
+    unsigned long long* __restrict__ exps, const T* __restrict__ sub_from, T* __restrict__ sub_out,
+    int sub_k, size_t img0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int CP = log_cp(C), SP = log_sp(C);
   T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
@@ -498,6 +501,8 @@ __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
   const bool full = (C & 3) == 0;
   T* outi = out + base;
   uint8_t* osi = SIGNED ? out_sign + base : nullptr;
+  const T* sfi = SUB ? sub_from + ((img0 + blockIdx.y) % (size_t)sub_k) * img_stride : nullptr;
+  T* soi = SUB ? sub_out + base : nullptr;
   unsigned n_ex = 0;  // exps evaluated by this thread (profiling only)
   // blockDim is a multiple of LR, so a thread keeps one row: rr = tid % LR,
   // groups tid / LR, tid / LR + 256 / LR, ...
@@ -516,6 +521,7 @@ __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
       for (int j = 0; j < 4; ++j) {
         outi[o + j * R] = v[j];
         if (SIGNED) osi[o + j * R] = pos[j] ? 1 : 0;
+        if (SUB) soi[o + j * R] = sfi[o + j * R] - v[j];
       }
     } else {
       const int nv = min(4, C - c0);
@@ -525,6 +531,7 @@ __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
         if (j < nv) {
           outi[o + j * R] = v[j];
           if (SIGNED) osi[o + j * R] = pos[j] ? 1 : 0;
+          if (SUB) soi[o + j * R] = sfi[o + j * R] - v[j];
         }
       }
     }
@@ -544,11 +551,13 @@ size_t log_axis_smem(int LR, int C) {
 
 template <typename T, int LR>
 int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
-                    const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+                    const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s, const T* sub_from,
+                    T* sub_out, int sub_k) {
   const size_t smem = log_axis_smem<T>(LR, C);
   if ((size_t)R * C >= (size_t)1 << 31)
     return set_error(ctx, WDL_ERR_UNSUPPORTED, "log-domain operator: image of 2^31 values or more");
   const T gamma_t = T(ctx->gamma);
+  unsigned long long* exps = ctx->profiling ? ctx->d_taps : nullptr;
   size_t done = 0;
   while (done < nimg) {
     size_t chunk = nimg - done;
@@ -556,15 +565,20 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
     dim3 grid((R + LR - 1) / LR, (unsigned)chunk);
     size_t off = done * img_stride;
     if (in_sign) {
-      auto k = log_axis_pass_kernel<T, true, LR>;
+      auto k = log_axis_pass_kernel<T, true, LR, false>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
-                                out_sign + off, ctx->profiling ? ctx->d_taps : nullptr);
-    } else {
-      auto k = log_axis_pass_kernel<T, false, LR>;
+                                out_sign + off, exps, nullptr, nullptr, 1, done);
+    } else if (sub_from) {
+      auto k = log_axis_pass_kernel<T, false, LR, true>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr,
-                                ctx->profiling ? ctx->d_taps : nullptr);
+      k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr, exps,
+                                sub_from, sub_out + off, sub_k, done);
+    } else {
+      auto k = log_axis_pass_kernel<T, false, LR, false>;
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr, exps,
+                                nullptr, nullptr, 1, done);
     }
     WDL_LAUNCH_CHECK(ctx);
     done += chunk;
@@ -574,12 +588,19 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
 
 template <typename T>
 int log_axis_dispatch(wdl_ctx* ctx, int LR, const T* in, T* out, int R, int C, size_t nimg,
-                      size_t img_stride, const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+                      size_t img_stride, const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s,
+                      const T* sub_from, T* sub_out, int sub_k) {
   // choice: rows per block
   switch (LR) {
-    case 8: return log_axis_launch<T, 8>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    case 16: return log_axis_launch<T, 16>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
-    default: return log_axis_launch<T, 32>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    case 8:
+      return log_axis_launch<T, 8>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from,
+                                   sub_out, sub_k);
+    case 16:
+      return log_axis_launch<T, 16>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from,
+                                    sub_out, sub_k);
+    default:
+      return log_axis_launch<T, 32>(ctx, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from,
+                                    sub_out, sub_k);
   }
 }
 
@@ -590,15 +611,16 @@ int log_axis_dispatch(wdl_ctx* ctx, int LR, const T* in, T* out, int R, int C, s
 // keeps the default.
 template <typename T>
 int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
-                  const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s) {
+                  const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s, const T* sub_from = nullptr,
+                  T* sub_out = nullptr, int sub_k = 1) {
   const long long key[6] = {1, R, C, (long long)nimg, (long long)sizeof(T), in_sign ? 1 : 0};
   for (const auto& e : ctx->tuned)
     if (!std::memcmp(e.key, key, sizeof(key)))
-      return log_axis_dispatch<T>(ctx, e.choice, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+      return log_axis_dispatch<T>(ctx, e.choice, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from, sub_out, sub_k);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
   if (!autotune_enabled() || !ctx->autotune || cap != cudaStreamCaptureStatusNone || ctx->profiling)
-    return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s);
+    return log_axis_dispatch<T>(ctx, kLogRowsDefault, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from, sub_out, sub_k);
   const int cand[3] = {8, 16, 32};
   int best = kLogRowsDefault;
   float best_ms = 1e30f;
@@ -609,9 +631,9 @@ int log_axis_pass(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, 
   for (int c : cand) {
     if (log_axis_smem<T>(c, C) > 200 * 1024) continue;
     // an untimed run first: the first launch of a variant also loads it
-    if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s))) break;
+    if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from, sub_out, sub_k))) break;
     cudaEventRecord(e0, s);
-    if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s))) break;
+    if ((rc = log_axis_dispatch<T>(ctx, c, in, out, R, C, nimg, img_stride, in_sign, out_sign, s, sub_from, sub_out, sub_k))) break;
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -695,7 +717,7 @@ int conv_stack_simt(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg, cuda
 template <typename T>
 int log_conv_stack_simt(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg,
                         const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                        cudaStream_t s) {
+                        cudaStream_t s, const T* sub_from, T* sub_out, size_t sub_period) {
   if (ctx->ndim != 2)
     return set_error(ctx, WDL_ERR_UNSUPPORTED, "log-domain operator is 2-D only (as the reference)");
   const int W = ctx->W, H = ctx->H;
@@ -704,7 +726,10 @@ int log_conv_stack_simt(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg,
   int rc;
   if ((rc = log_axis_pass<T>(ctx, in, tmp, H, W, nimg, N, in_sign, in_sign ? tmp_sign : nullptr, s)))
     return rc;
-  if ((rc = log_axis_pass<T>(ctx, tmp, out, W, H, nimg, N, in_sign ? tmp_sign : nullptr, out_sign, s)))
+  if (sub_from && (in_sign || sub_period == 0 || sub_period % N))
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "log_conv_stack: subtraction needs an unsigned operand and whole images");
+  if ((rc = log_axis_pass<T>(ctx, tmp, out, W, H, nimg, N, in_sign ? tmp_sign : nullptr, out_sign, s,
+                             sub_from, sub_out, sub_from ? (int)(sub_period / N) : 1)))
     return rc;
   timer.done();
   return WDL_OK;
@@ -724,14 +749,16 @@ int conv_stack_simt_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, s
 
 int log_conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
                        const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                       cudaStream_t s) {
-  return log_conv_stack_simt<float>(ctx, in, out, tmp, nimg, in_sign, out_sign, tmp_sign, s);
+                       cudaStream_t s, const float* sub_from, float* sub_out, size_t sub_period) {
+  return log_conv_stack_simt<float>(ctx, in, out, tmp, nimg, in_sign, out_sign, tmp_sign, s, sub_from,
+                                    sub_out, sub_period);
 }
 
 int log_conv_stack_f64(wdl_ctx* ctx, const double* in, double* out, double* tmp, size_t nimg,
                        const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                       cudaStream_t s) {
-  return log_conv_stack_simt<double>(ctx, in, out, tmp, nimg, in_sign, out_sign, tmp_sign, s);
+                       cudaStream_t s, const double* sub_from, double* sub_out, size_t sub_period) {
+  return log_conv_stack_simt<double>(ctx, in, out, tmp, nimg, in_sign, out_sign, tmp_sign, s, sub_from,
+                                     sub_out, sub_period);
 }
 
 }  // namespace wdl

@@ -186,17 +186,6 @@ __global__ void k_poison_out_of_range(T* __restrict__ bary, const int* __restric
 }
 
 // ---------------- log-domain forward (:700-720, :167-196) ---------------------------
-// Thread per dictionary entry q, histograms p in order (no index division).
-template <typename T>
-__global__ void k_log_sub_atoms(const T* __restrict__ log_atoms, const T* __restrict__ cb,
-                                T* __restrict__ a, size_t KN, int P) {
-  GRID_STRIDE(q, KN) {
-    const T lp = log_atoms[q];
-#pragma unroll 4
-    for (int p = 0; p < P; ++p) a[(size_t)p * KN + q] = lp - cb[(size_t)p * KN + q];
-  }
-}
-
 template <typename T>
 __global__ void k_log_bary_b(const T* __restrict__ phi, const T* __restrict__ lam,
                              T* __restrict__ b, T* __restrict__ bary_log, int K, size_t N,
@@ -764,11 +753,10 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       if ((rc = conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, s))) return rc;
       k_bary_b<T><<<G_PN, 256, 0, s>>>(phi, B.lam64, b_next, B.bary, K, N, PN, range);
     } else {
+      // cb = conv(b_prev), and a = log atoms - cb from the same pass
       if ((rc = log_conv_stack<T>(ctx, b_prev, cb, B.ctmp, (size_t)P * K, nullptr, nullptr,
-                                  nullptr, s)))
+                                  nullptr, s, B.atoms, B.a, KN)))
         return rc;
-      k_log_sub_atoms<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.atoms, cb, B.a, KN, P);
-      WDL_LAUNCH_CHECK(ctx);
       if ((rc = log_conv_stack<T>(ctx, B.a, phi, B.ctmp, (size_t)P * K, nullptr, nullptr,
                                   nullptr, s)))
         return rc;
@@ -931,10 +919,9 @@ int barycenter_t(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const d
       if ((rc = conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, s))) return rc;
       k_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam64, b, bary, K, N, PN, range);
     } else {
-      if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
+      if ((rc = log_conv_stack<T>(ctx, b, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s, at, a,
+                                  KN)))
         return rc;
-      k_log_sub_atoms<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(at, conv, a, KN, (int)(PKN / KN));
-      WDL_LAUNCH_CHECK(ctx);
       if ((rc = log_conv_stack<T>(ctx, a, conv, tmp, (size_t)P * K, nullptr, nullptr, nullptr, s)))
         return rc;
       k_log_bary_b<T><<<launch_cfg(ctx, PN), 256, 0, s>>>(conv, lam, b, bary, K, N, PN);

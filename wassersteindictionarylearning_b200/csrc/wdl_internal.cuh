@@ -165,13 +165,17 @@ int conv_stack_f64(wdl_ctx* ctx, const double* in, double* out, double* tmp, siz
 int conv_stack_simt_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
                         cudaStream_t s);
 // Log-sum-exp operator; signs (one byte per element, 1 = non-negative) are read
-// from in_sign and written to out_sign when non-null.
+// from in_sign and written to out_sign when non-null.  With sub_from non-null
+// (unsigned only) the last pass also writes sub_out[i] = sub_from[i mod
+// sub_period] - out[i] for every element i of the nimg images.
 int log_conv_stack_f32(wdl_ctx* ctx, const float* in, float* out, float* tmp, size_t nimg,
                        const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                       cudaStream_t s);
+                       cudaStream_t s, const float* sub_from = nullptr, float* sub_out = nullptr,
+                       size_t sub_period = 0);
 int log_conv_stack_f64(wdl_ctx* ctx, const double* in, double* out, double* tmp, size_t nimg,
                        const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                       cudaStream_t s);
+                       cudaStream_t s, const double* sub_from = nullptr, double* sub_out = nullptr,
+                       size_t sub_period = 0);
 
 template <typename T>
 inline int conv_stack(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg, cudaStream_t s);
@@ -189,18 +193,19 @@ inline int conv_stack<double>(wdl_ctx* ctx, const double* in, double* out, doubl
 template <typename T>
 inline int log_conv_stack(wdl_ctx* ctx, const T* in, T* out, T* tmp, size_t nimg,
                           const uint8_t* in_sign, uint8_t* out_sign, uint8_t* tmp_sign,
-                          cudaStream_t s);
+                          cudaStream_t s, const T* sub_from = nullptr, T* sub_out = nullptr,
+                          size_t sub_period = 0);
 template <>
 inline int log_conv_stack<float>(wdl_ctx* ctx, const float* in, float* out, float* tmp,
                                  size_t nimg, const uint8_t* is, uint8_t* os, uint8_t* ts,
-                                 cudaStream_t s) {
-  return log_conv_stack_f32(ctx, in, out, tmp, nimg, is, os, ts, s);
+                                 cudaStream_t s, const float* sf, float* so, size_t sp) {
+  return log_conv_stack_f32(ctx, in, out, tmp, nimg, is, os, ts, s, sf, so, sp);
 }
 template <>
 inline int log_conv_stack<double>(wdl_ctx* ctx, const double* in, double* out, double* tmp,
                                   size_t nimg, const uint8_t* is, uint8_t* os, uint8_t* ts,
-                                  cudaStream_t s) {
-  return log_conv_stack_f64(ctx, in, out, tmp, nimg, is, os, ts, s);
+                                  cudaStream_t s, const double* sf, double* so, size_t sp) {
+  return log_conv_stack_f64(ctx, in, out, tmp, nimg, is, os, ts, s, sf, so, sp);
 }
 
 // Tensor-core resources (conv_tc.cu).
