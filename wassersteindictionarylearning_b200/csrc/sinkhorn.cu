@@ -35,6 +35,20 @@ template <>
 __device__ __forceinline__ float d_log<float>(float x) { return logf(x); }
 template <>
 __device__ __forceinline__ double d_log<double>(double x) { return log(x); }
+// Natural log of a magnitude feeding a log-domain operand: FP32 takes the
+// hardware base-2 logarithm times ln 2 (absolute error ~2e-7, i.e. ~2e-7
+// relative on the scaling it encodes; a log-domain value of magnitude >= 2 is
+// rounded more coarsely than that anyway); FP64 the library log.
+template <typename T>
+__device__ __forceinline__ T d_log_mag(T x);
+template <>
+__device__ __forceinline__ float d_log_mag<float>(float x) {
+  float y;
+  asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(fabsf(x)));
+  return y * 0.6931471805599453f;
+}
+template <>
+__device__ __forceinline__ double d_log_mag<double>(double x) { return log(fabs(x)); }
 
 // safe_log = log(max(EPSILON, x)) (cpp/loss.h:3-5).
 template <typename T>
@@ -527,11 +541,11 @@ __global__ void __launch_bounds__(1024) k_lbwd_post_pre(
         const size_t i = ib + j;
         const T x = l * sn + vv[h];
         sd[i] = x >= T(0);
-        tmp[i] = d_log<T>(fabs(x)) + cur.bp[h];
+        tmp[i] = d_log_mag<T>(x) + cur.bp[h];
         acc += (double)cur.ph[h] * (double)sg;
         const T y = l * sg + rr[h];
         sw[i] = y >= T(0);
-        u[i] = d_log<T>(fabs(y)) - cur.ph[h];
+        u[i] = d_log_mag<T>(y) - cur.ph[h];
       }
     }
     __syncthreads();
