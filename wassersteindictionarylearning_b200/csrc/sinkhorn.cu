@@ -1152,6 +1152,9 @@ int replay_or_run(wdl_ctx* ctx, const unsigned long long (&key)[20], cudaStream_
   if (ctx->profiling || ctx->trace_level || s == nullptr || s == cudaStreamLegacy ||
       s == cudaStreamPerThread)
     return run();
+  // inside a caller's own capture the call becomes part of that graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return run();
   wdl_ctx::GraphEntry* e = nullptr;
   for (auto& g : ctx->graphs)
     if (!std::memcmp(g.key, key, sizeof(key))) e = &g;
@@ -1230,8 +1233,19 @@ int gradient_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, const do
 int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
                    double* bary, cudaStream_t s) {
   if (use_fused(ctx, WDL_LOSS_QUADRATIC)) return barycenter_fused(ctx, P, K, L, atoms, weights, bary, s);
-  if (use_fp64(ctx)) return barycenter_t<double>(ctx, P, K, L, atoms, weights, bary, s);
-  return barycenter_t<float>(ctx, P, K, L, atoms, weights, bary, s);
+  // replayed like gradient_both_dev (a request loop repeats the same call);
+  // the workspace is sized before the key is formed
+  int rc;
+  if ((rc = ensure_arena(ctx, barycenter_bytes(ctx, P, K)))) return rc;
+  const unsigned long long key[20] = {
+      2ull, (unsigned long long)P, (unsigned long long)K, (unsigned long long)L, 0ull, 0ull,
+      (unsigned long long)(uintptr_t)atoms, (unsigned long long)(uintptr_t)weights, 0ull, 0ull,
+      (unsigned long long)(uintptr_t)bary, 0ull, 0ull, 0ull, 0ull, (unsigned long long)(uintptr_t)s,
+      (unsigned long long)(uintptr_t)ctx->arena.ptr, (unsigned long long)ctx->arena.bytes, 0ull, 0ull};
+  return replay_or_run(ctx, key, s, [&]() {
+    if (use_fp64(ctx)) return barycenter_t<double>(ctx, P, K, L, atoms, weights, bary, s);
+    return barycenter_t<float>(ctx, P, K, L, atoms, weights, bary, s);
+  });
 }
 
 // evaluate_both (cpp/inverseWasserstein.h:986-1145) on device.  The gradient_both

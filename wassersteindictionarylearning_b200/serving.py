@@ -392,6 +392,30 @@ class ServingEngine:
                 if fast is not None:
                     self._side.submit(fast.kernel.close)
 
+    def capture_graphs(self, batch_headroom: int = 2):
+        """Record each resident shape's one-request projection and barycenter
+        calls as CUDA graphs before serving.  A context replays a call whose
+        sizes, buffers and stream it has seen twice (the first runs eagerly,
+        the second is captured); those first two runs are ~1000 separate
+        launches each, which a request loop on many shapes would otherwise pay
+        on nearly every request.  A batch_headroom-request call first sizes the
+        context's buffers, so that batches up to that size do not move them
+        (which would retire the recorded graphs)."""
+        K, L = self.K, self.L
+        for s in list(self._shapes.values()):
+            ctx, N = s.kernel.ctx, s.kernel.N
+            atoms = f64(s.atoms)
+            obs1 = f64(s.atoms.reshape(K, N)[0])
+            for P in (batch_headroom, 1, 1):
+                lam = f64(np.full((P, K), 1.0 / K))
+                obs = f64(np.tile(obs1, P))
+                la, loss = np.empty(P * K), np.empty(P)
+                check(lib().wdl_gradient_both(ctx, P, K, L, self.loss_type, dptr(atoms), dptr(lam),
+                                              dptr(obs), None, dptr(la), None, None, dptr(loss), None), ctx)
+            w, out = f64(np.full(K, 1.0 / K)), np.empty(N)
+            for _ in range(2):
+                check(lib().wdl_barycenter(ctx, 1, K, L, dptr(atoms), dptr(w), dptr(out)), ctx)
+
     def warm_up(self):
         """Serve one barycenter and one projection request per operator form
         (2-D grid up to 128, 2-D grid above 128, 3-D volume; fast and FP64) on
