@@ -115,3 +115,25 @@ def test_fp32_overflow_is_served_in_fp64():
     cal.preload([shape])
     assert shape in cal.wide_shapes
     cal.close()
+
+
+def test_recorded_graphs_serve_the_same_results():
+    """capture_graphs() records every resident shape's one-request projection
+    and barycenter calls as CUDA graphs; requests served afterwards (replays)
+    return bitwise what an engine without recorded graphs returns (FP64)."""
+    import copy
+    arr = _stream(10, seed=5, frac_3d=0.3)
+    shapes = sorted({req.shape for _, req in arr})
+    results = []
+    for record in (False, True):
+        eng = _engine("fp64")
+        eng.preload(shapes, calibrate=False)
+        if record:
+            eng.capture_graphs()
+        done = sorted(eng.run(copy.deepcopy(arr)), key=lambda r: r.rid)
+        eng.close()
+        assert len(done) == 10 and all(r.status == 0 for r in done)
+        results.append(done)
+    for a, b in zip(*results):
+        assert a.kind == b.kind and a.shape == b.shape
+        assert np.array_equal(a.result, b.result), (a.kind, a.shape)
