@@ -479,12 +479,15 @@ __host__ __device__ constexpr int log_sp(int C) { return C + 2 * kHalo + 4; }
 // consecutive rows.
 // SUB: also write sub_out = sub_from (period sub_k images) - out, image by
 // image (img0: the launch's first image).
-template <typename T, bool SIGNED, int LR, bool SUB>
+// SQ > 0: the images are SQ x SQ (R = C = SQ), known at compile time, so
+// strides and loop bounds are constants.
+template <typename T, bool SIGNED, int LR, bool SUB, int SQ>
 __global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
-    const T* __restrict__ in, T* __restrict__ out, int R, int C, size_t img_stride, T gamma_t,
+    const T* __restrict__ in, T* __restrict__ out, int R_, int C_, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
     unsigned long long* __restrict__ exps, const T* __restrict__ sub_from, T* __restrict__ sub_out,
     int sub_k, size_t img0) {
+  const int R = SQ > 0 ? SQ : R_, C = SQ > 0 ? SQ : C_;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int CP = log_cp(C), SP = log_sp(C);
   T* rows = reinterpret_cast<T*>(smem_raw);             // [LR][CP]
@@ -549,6 +552,10 @@ size_t log_axis_smem(int LR, int C) {
   return ((size_t)LR * log_cp(C) + C + LR) * sizeof(T) + (size_t)LR * log_sp(C) + 16;
 }
 
+// The grid side compiled as a constant (the log-domain dictionary-learning
+// configuration's 256 x 256); other shapes take the general kernel.
+constexpr int kLogSquare = 256;
+
 template <typename T, int LR>
 int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg, size_t img_stride,
                     const uint8_t* in_sign, uint8_t* out_sign, cudaStream_t s, const T* sub_from,
@@ -564,18 +571,19 @@ int log_axis_launch(wdl_ctx* ctx, const T* in, T* out, int R, int C, size_t nimg
     if (chunk > 65535) chunk = 65535;
     dim3 grid((R + LR - 1) / LR, (unsigned)chunk);
     size_t off = done * img_stride;
+    const bool sq = R == kLogSquare && C == kLogSquare;
     if (in_sign) {
-      auto k = log_axis_pass_kernel<T, true, LR, false>;
+      auto k = sq ? log_axis_pass_kernel<T, true, LR, false, kLogSquare> : log_axis_pass_kernel<T, true, LR, false, 0>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, in_sign + off,
                                 out_sign + off, exps, nullptr, nullptr, 1, done);
     } else if (sub_from) {
-      auto k = log_axis_pass_kernel<T, false, LR, true>;
+      auto k = sq ? log_axis_pass_kernel<T, false, LR, true, kLogSquare> : log_axis_pass_kernel<T, false, LR, true, 0>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr, exps,
                                 sub_from, sub_out + off, sub_k, done);
     } else {
-      auto k = log_axis_pass_kernel<T, false, LR, false>;
+      auto k = sq ? log_axis_pass_kernel<T, false, LR, false, kLogSquare> : log_axis_pass_kernel<T, false, LR, false, 0>;
       if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k<<<grid, 256, smem, s>>>(in + off, out + off, R, C, img_stride, gamma_t, nullptr, nullptr, exps,
                                 nullptr, nullptr, 1, done);
