@@ -213,6 +213,22 @@ typedef struct {
 } wdl_fit_problem;
 int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* problems, int nproblems, int max_iterations,
                     double epsilon);
+/* The same fits (same transform, algorithm, constants and status codes) for
+ * P histograms on the context's own grid with the context's own evaluation:
+ * any dimension (2-D or 3-D), precision and domain the context computes,
+ * except the fused tensor-core form (use wdl_fit_weights there).  Every round
+ * is one weights-only compute_gradient_both over the P histograms followed by
+ * one step of every optimisation on the device; the rounds after the first
+ * are one CUDA graph, and the host reads the done flags every few rounds.
+ * Histograms that finished are evaluated along at their last point without
+ * moving.  Host buffers: atoms [K*N], observed [P*N], x0 [P*K] or NULL;
+ * outputs weights [P*K], loss [P], status [P], evaluations [P].  A non-finite
+ * evaluation ends that fit with WDL_ERR_NONFINITE.  The reference's
+ * counterpart is regress_both with the atoms held fixed, one histogram at a
+ * time on the host. */
+int wdl_fit_weights_operator(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                             const double* observed, const double* x0, int max_iterations, double epsilon,
+                             double* weights, double* loss, int* status, int* evaluations);
 /* The same fit in the LOG domain (compute_gradient_both_log_signArray,
  * cpp/inverseWasserstein.h:678-814, restricted to the forward pass, the loss
  * and the weight recursion), for problems whose kernel-domain scalings leave

@@ -137,3 +137,24 @@ def test_recorded_graphs_serve_the_same_results():
     for a, b in zip(*results):
         assert a.kind == b.kind and a.shape == b.shape
         assert np.array_equal(a.result, b.result), (a.kind, a.shape)
+
+
+def test_device_fit_serves_the_host_fits():
+    """With device_fit the FP64 projections run wdl_fit_weights_operator (the
+    L-BFGS on the device) and return the host L-BFGS's weights."""
+    import copy
+    arr = _stream(8, seed=9, frac_3d=0.3)
+    outs = []
+    for device_fit in (False, True):
+        eng = _engine("fp64", device_fit=device_fit)
+        done = sorted(eng.run(copy.deepcopy(arr)), key=lambda r: r.rid)
+        eng.close()
+        assert len(done) == 8 and all(r.status == 0 for r in done)
+        outs.append(done)
+    for a, b in zip(*outs):
+        assert a.kind == b.kind and a.shape == b.shape
+        if a.kind == "projection":
+            assert a.lbfgs_status == b.lbfgs_status
+            assert np.max(np.abs(a.result - b.result)) < 1e-8
+        else:
+            assert np.array_equal(a.result, b.result)

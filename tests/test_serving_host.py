@@ -35,8 +35,9 @@ class _Kernel:
 class _FakeLib:
     """numpy model of wdl_barycenter / wdl_gradient_both (weights only)."""
 
-    def __init__(self, out_of_range=(), slow=(), delay=0.0):
+    def __init__(self, out_of_range=(), slow=(), delay=0.0, device_fit=False):
         self.out_of_range, self.slow, self.delay = set(out_of_range), set(slow), delay
+        self.device_fit = device_fit
         self.calls = []
         self.lock = threading.Lock()
 
@@ -83,6 +84,29 @@ class _FakeLib:
             g[:], f[:] = np.nan, np.nan
         self._view(la, P * K)[:] = g.reshape(-1)
         self._view(loss, P)[:] = f
+        return 0
+
+    def wdl_fit_weights_operator(self, ctx, P, K, L, loss_type, atoms, obs, x0, iters, eps, w, loss,
+                                 status, evals):
+        """-4 (unsupported: the fused tensor-core answer) unless device_fit; then
+        a whole fit in one call: the least-squares weights of the numpy model,
+        or status -5 (non-finite) where the model leaves the range."""
+        if not self.device_fit:
+            return -4
+        self._log(ctx, "fit", P)
+        N = ctx.N
+        a = self._view(atoms, K * N).reshape(K, N)
+        ob = self._view(obs, P * N).reshape(P, N)
+        wv, fv = self._view(w, P * K).reshape(P, K), self._view(loss, P)
+        st = np.ctypeslib.as_array(status, shape=(P,))
+        ev = np.ctypeslib.as_array(evals, shape=(P,))
+        for p in range(P):
+            x = np.clip(np.linalg.lstsq(a.T, ob[p], rcond=None)[0], 0, None) + 1e-12
+            wv[p] = x / x.sum()
+            d = wv[p] @ a - ob[p]
+            fv[p] = d @ d
+            st[p] = -5 if self._bad(ctx) else 0
+            ev[p] = iters + 1
         return 0
 
 
@@ -191,3 +215,21 @@ def test_admission_holds_requests_beyond_the_budget(fake):
     assert len(done) == len(reqs) and all(r.status == 0 for r in done)
     assert max(peak) <= 1.5 * b and eng.admitted_bytes == 0
     assert [r.rid for r in done] == sorted(r.rid for r in done)  # served in arrival order
+
+
+def test_device_fits_serve_projections_in_one_call(fake):
+    """With the device fit available, a shape batch's projections finish in one
+    wdl_fit_weights_operator call; a fast-form fit that leaves the range starts
+    over in FP64 and is fitted there."""
+    lib = fake(out_of_range={(6, 5, 1)}, device_fit=True)
+    eng = _engine(device_fit=True)
+    arr = [(0.0, r) for _, r in _requests([(6, 5, 1), (4, 4, 1), (6, 5, 1), (3, 3, 2)], seed=4)]
+    done = sorted(eng.run(arr), key=lambda r: r.rid)
+    eng.close()
+    assert len(done) == 4 and all(r.status == 0 for r in done)
+    fits = [c for c in lib.calls if c[2] == "fit"]
+    assert not [c for c in lib.calls if c[2] == "grad"]  # no host L-BFGS evaluations
+    assert ((6, 5, 1), "fp64") in {(c[0], c[1]) for c in fits}  # the escalated projection
+    for r in done:
+        if r.kind == serving.PROJECTION:
+            assert r.result.shape == (3,) and abs(r.result.sum() - 1) < 1e-12 and r.lbfgs_status == 0

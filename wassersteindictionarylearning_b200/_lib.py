@@ -92,6 +92,8 @@ SIGNATURES = {
     "wdl_batch_run": ([_vp, C.c_void_p, C.c_int], C.c_int),
     "wdl_fit_weights": ([_vp, C.c_void_p, C.c_int, C.c_int, C.c_double], C.c_int),
     "wdl_fit_weights_log": ([_vp, C.c_void_p, C.c_int, C.c_int, C.c_double], C.c_int),
+    "wdl_fit_weights_operator": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int,
+                                  C.c_double, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "wdl_launch_count": ([_vp], C.c_longlong),
     "wdl_set_profiling": ([_vp, C.c_int], C.c_int),
     "wdl_conv_profile": ([_vp, _dp, C.POINTER(C.c_longlong), _dp], C.c_int),

@@ -69,6 +69,19 @@ __global__ void k_fit_round(LbOpt* opts, int n, LbParam prm, const int* fused_sy
   done[i] = o.s.phase == 2 ? 1 : 0;
 }
 
+// k_fit_round with the L-BFGS settings read from device memory, so that a
+// recorded round does not depend on them.
+__global__ void k_fit_round_dp(LbOpt* opts, int n, const LbParam* prm, uint8_t* done) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  LbOpt o = opts[i];
+  if (o.s.phase == 2) return;
+  const LbParam pv = *prm;
+  lbfgs_advance(o.s, o.v, o.loss[0], o.dot, o.lam64, o.lam32, pv, WDL_FIT_OVERFLOW);
+  opts[i] = o;
+  done[i] = o.s.phase == 2 ? 1 : 0;
+}
+
 struct FitOut {
   double w[64];
   double loss;
@@ -268,6 +281,134 @@ extern "C" int wdl_fit_weights(wdl_ctx* ctx, const wdl_fit_problem* fp, int npro
       f.status[p] = h_out[i].status;
       f.evaluations[p] = h_out[i].evals;
     }
+  }
+  return WDL_OK;
+}
+
+// wdl_fit_weights_operator: the fits of wdl_fit_weights for P histograms on the
+// context's own grid and evaluation path.  Round r evaluates the P histograms
+// at their current trial points (gradient_both_dev, weights only: the weight
+// gradient resultLa and the loss) and k_fit_round advances every optimisation.
+// The first round runs eagerly (it sizes the context's workspace); the next
+// ones are captured once and replayed.
+extern "C" int wdl_fit_weights_operator(wdl_ctx* ctx, int P, int K, int L, int loss_type, const double* atoms,
+                                        const double* observed, const double* x0, int max_iterations,
+                                        double epsilon, double* weights, double* loss, int* status,
+                                        int* evaluations) {
+  if (!ctx) return WDL_ERR_INVALID_ARG;
+  if (P < 1 || K < 1 || K > 64 || L < 1 || max_iterations < 0 || !(epsilon >= 0) || !atoms || !observed ||
+      !weights || !loss || !status || !evaluations)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "bad sizes or NULL required pointer");
+  if (loss_type < WDL_LOSS_TV || loss_type > WDL_LOSS_KL)
+    return set_error(ctx, WDL_ERR_INVALID_ARG, "loss_type must be 1..4");
+  if (tc_fused(ctx) && ctx->domain == WDL_DOMAIN_KERNEL && loss_type != WDL_LOSS_WASSERSTEIN)
+    return set_error(ctx, WDL_ERR_UNSUPPORTED, "fused tensor-core context: use wdl_fit_weights");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(ctx, WDL_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = ctx->stream;
+  const size_t N = ctx->N, KN = (size_t)K * N, PK = (size_t)P * K, PN = (size_t)P * N;
+  // device layout: atoms, observed, weights under evaluation, resultLa, loss,
+  // optimiser table and state pool, starting points, outputs, done flags, a
+  // zeroed word pair standing for the fused kernel's error flag
+  ArenaPlan plan;
+  plan.take<double>(KN);
+  plan.take<double>(PN);
+  plan.take<double>(PK);
+  plan.take<double>(PK);
+  plan.take<double>(P);
+  plan.take<LbOpt>(P);
+  plan.take<double>((size_t)P * pool_doubles(K));
+  plan.take<double>((size_t)P * 64);
+  plan.take<FitOut>(P);
+  plan.take<uint8_t>(P);
+  plan.take<LbParam>(1);
+  Arena& A = ctx->lbfgs_arena;
+  if (plan.off + 256 > A.bytes) {
+    WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    if (A.ptr) WDL_CUDA_TRY(ctx, cudaFree(A.ptr));
+    A.ptr = nullptr;
+    A.bytes = 0;
+    WDL_CUDA_TRY(ctx, cudaMalloc(&A.ptr, plan.off + 256));
+    A.bytes = plan.off + 256;
+  }
+  A.reset();
+  double* d_atoms = A.take<double>(KN);
+  double* d_obs = A.take<double>(PN);
+  double* d_lam = A.take<double>(PK);
+  double* d_la = A.take<double>(PK);
+  double* d_loss = A.take<double>(P);
+  LbOpt* d_opts = A.take<LbOpt>(P);
+  double* d_pool = A.take<double>((size_t)P * pool_doubles(K));
+  double* d_x0 = A.take<double>((size_t)P * 64);
+  FitOut* d_out = A.take<FitOut>(P);
+  uint8_t* d_done = A.take<uint8_t>(P);
+  LbParam* d_prm = A.take<LbParam>(1);
+  std::vector<LbOpt> opts(P);
+  std::vector<double> h_x0((size_t)P * 64, 0.0);
+  for (int p = 0; p < P; ++p) {
+    LbOpt o{};
+    o.s.K = K;
+    o.v = d_pool + (size_t)p * pool_doubles(K);
+    o.lam64 = d_lam + (size_t)p * K;
+    o.lam32 = nullptr;
+    o.dot = d_la + (size_t)p * K;
+    o.loss = d_loss + p;
+    opts[p] = o;
+    if (x0)
+      for (int k = 0; k < K; ++k) h_x0[(size_t)p * 64 + k] = x0[(size_t)p * K + k];
+  }
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_atoms, atoms, KN * 8, cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_obs, observed, PN * 8, cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_opts, opts.data(), P * sizeof(LbOpt), cudaMemcpyHostToDevice, s));
+  if (x0) WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_x0, h_x0.data(), h_x0.size() * 8, cudaMemcpyHostToDevice, s));
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(d_done, 0, P, s));
+  const LbParam prm{max_iterations, 20, epsilon, 1e-4, 0.9, 1e-20, 1e20};
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(d_prm, &prm, sizeof(prm), cudaMemcpyHostToDevice, s));
+  const unsigned og = (unsigned)((P + 127) / 128);
+  k_fit_init<<<og, 128, 0, s>>>(d_opts, P, x0 ? d_x0 : nullptr);
+  WDL_LAUNCH_CHECK(ctx);
+  const long long max_rounds = (long long)(max_iterations > 0 ? max_iterations : 1000) * (prm.max_linesearch + 1) + 2;
+  // one round: the evaluation of every histogram, then one step of each fit
+  auto round = [&]() -> int {
+    int rc = gradient_both_dev(ctx, P, K, L, loss_type, d_atoms, d_lam, d_obs, nullptr, d_la, nullptr, nullptr,
+                               d_loss, nullptr, s, true);
+    if (rc) return rc;
+    k_fit_round_dp<<<og, 128, 0, s>>>(d_opts, P, d_prm, d_done);
+    WDL_LAUNCH_CHECK(ctx);
+    return WDL_OK;
+  };
+  // Rounds go through the context's graph cache: the workspace is sized first,
+  // so a later call with the same sizes (whatever its L-BFGS settings, which
+  // the round reads from device memory) replays the same recorded round from
+  // its first round on.
+  int rc = ensure_arena(ctx, eval_bytes(ctx, P, K, L));
+  if (rc) return rc;
+  const unsigned long long key[20] = {
+      3ull, (unsigned long long)P, (unsigned long long)K, (unsigned long long)L, (unsigned long long)loss_type,
+      0ull, 0ull, (unsigned long long)(uintptr_t)A.ptr,
+      (unsigned long long)A.bytes, (unsigned long long)(uintptr_t)s, (unsigned long long)(uintptr_t)ctx->arena.ptr,
+      (unsigned long long)ctx->arena.bytes, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+  const int chunk = 4;  // rounds between looks at the done flags
+  std::vector<uint8_t> h_done(P, 0);
+  long long rounds = 0;
+  while (rounds < max_rounds) {
+    for (int r = 0; r < chunk && rounds < max_rounds; ++r, ++rounds)
+      if ((rc = replay_or_run(ctx, key, s, round)) != WDL_OK) return rc;
+    WDL_CUDA_TRY(ctx, cudaMemcpyAsync(h_done.data(), d_done, P, cudaMemcpyDeviceToHost, s));
+    WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    bool all = true;
+    for (uint8_t d : h_done) all = all && d;
+    if (all) break;
+  }
+  k_fit_outputs<<<og, 128, 0, s>>>(d_opts, P, d_out);
+  WDL_LAUNCH_CHECK(ctx);
+  std::vector<FitOut> h_out(P);
+  WDL_CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), d_out, P * sizeof(FitOut), cudaMemcpyDeviceToHost, s));
+  WDL_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  for (int p = 0; p < P; ++p) {
+    for (int k = 0; k < K; ++k) weights[(size_t)p * K + k] = h_out[p].w[k];
+    loss[p] = h_out[p].loss;
+    status[p] = h_out[p].status == WDL_FIT_OVERFLOW ? WDL_ERR_NONFINITE : h_out[p].status;
+    evaluations[p] = h_out[p].evals;
   }
   return WDL_OK;
 }

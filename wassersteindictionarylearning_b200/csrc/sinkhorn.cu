@@ -1166,7 +1166,7 @@ int replay_or_run(wdl_ctx* ctx, const unsigned long long (&key)[20], cudaStream_
   if (!e) {  // first sighting: eager
     const int rc = run();
     if (rc) return rc;
-    if (ctx->graphs.size() >= 8) {
+    if (ctx->graphs.size() >= 16) {
       if (ctx->graphs.front().exec) cudaGraphExecDestroy(ctx->graphs.front().exec);
       ctx->graphs.erase(ctx->graphs.begin());
     }

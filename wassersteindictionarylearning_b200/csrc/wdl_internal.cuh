@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -309,6 +310,12 @@ int evaluate_both_dev(wdl_ctx* ctx, int P, int K, int L, int loss_type, double s
 int barycenter_dev(wdl_ctx* ctx, int P, int K, int L, const double* atoms, const double* weights,
                    double* bary, cudaStream_t s);
 size_t eval_bytes(const wdl_ctx* ctx, int P, int K, int L);
+// Runs `run` (a fixed sequence of launches on s) eagerly the first time a key
+// is seen, captures it into a CUDA graph the second time and replays the graph
+// afterwards (sinkhorn.cu); inside a caller's capture it just runs.  The key
+// must name every size, pointer and parameter the launches depend on.
+int replay_or_run(wdl_ctx* ctx, const unsigned long long (&key)[20], cudaStream_t s,
+                  const std::function<int()>& run);
 size_t barycenter_bytes(const wdl_ctx* ctx, int P, int K);
 
 }  // namespace wdl

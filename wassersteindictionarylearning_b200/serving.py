@@ -70,6 +70,7 @@ class _Shape:
     kernel: object
     atoms: np.ndarray
     active: list = field(default_factory=list)
+    device_fit: bool = True  # cleared when the context's form has no device fit (fused tensor-core)
 
 
 class ServingEngine:
@@ -88,7 +89,7 @@ class ServingEngine:
                  precision: str = "split_bf16", hbm_budget: float = 8e9, max_batch: int = 64,
                  lbfgs_iterations: int = 20, max_shapes: int = 512, workers: int = 8,
                  dictionary_seed: int = 100, device: int = 0, autotune: bool = False,
-                 lbfgs_epsilon: float = 1e-50):
+                 lbfgs_epsilon: float = 1e-50, device_fit: bool = False):
         self.K, self.L, self.gamma, self.loss_type = K, L, gamma, loss_type
         self.precision = precision
         self.hbm_budget = hbm_budget
@@ -99,6 +100,13 @@ class ServingEngine:
         self.lbfgs_param = lb.LbfgsParam(max_iterations=lbfgs_iterations, epsilon=lbfgs_epsilon)
         self.max_shapes = max_shapes
         self.device = device
+        # device_fit: projections on the CUDA-core forms (FP64, 3-D FP32) fit
+        # their weights with the L-BFGS on the device (wdl_fit_weights_operator):
+        # one call per shape batch instead of one host round trip per
+        # evaluation, but a fit holds its shape until it ends, so requests that
+        # arrive meanwhile no longer join the running batch (off by default:
+        # the host loop served the bench mix at a higher rate)
+        self.device_fit = device_fit
         self.dictionary_seed = dictionary_seed
         # a request loop keeps the default launch variants: timing variants on a
         # shape's first calls would add synchronisations to those requests
@@ -306,6 +314,8 @@ class ServingEngine:
                 r.status = rc_i
                 r.result = res.copy() if rc_i == 0 else None
                 self._finish(s, r)
+        if proj_reqs and self.device_fit and s.device_fit and self._fit_on_device(s, proj_reqs, fast):
+            proj_reqs = []
         if proj_reqs:
             P = len(proj_reqs)
             # x = log-weights; lambda = normalise(exp(x)) (evaluate_both's transform, :997-1020)
@@ -348,6 +358,52 @@ class ServingEngine:
                     # only a cancellation (NaN objective) fails the request.
                     r.status = lb.LBFGSERR_CANCELED if status == lb.LBFGSERR_CANCELED else 0
                     self._finish(s, r)
+
+    def _fit_call(self, s: _Shape, obs: np.ndarray, max_iterations: int):
+        """wdl_fit_weights_operator over the rows of obs on the shape's context:
+        (rc, weights [P*K], loss [P], status [P])."""
+        import ctypes as C
+        K, L = self.K, self.L
+        P = obs.shape[0]
+        obs = f64(obs.reshape(-1))
+        w, f = np.empty(P * K), np.empty(P)
+        st, ev = np.zeros(P, dtype=np.int32), np.zeros(P, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        rc = lib().wdl_fit_weights_operator(s.kernel.ctx, P, K, L, self.loss_type, dptr(f64(s.atoms)), dptr(obs),
+                                            None, max_iterations, self.lbfgs_param.epsilon, dptr(w), dptr(f),
+                                            st.ctypes.data_as(ip), ev.ctypes.data_as(ip))
+        return rc, w, f, st
+
+    def _fit_on_device(self, s: _Shape, reqs, fast: bool) -> bool:
+        """Fit every projection request of the batch to completion in one
+        wdl_fit_weights_operator call (regress_both's L-BFGS with the atoms
+        fixed, on the device, from uniform weights).  False when the shape's
+        form has no device fit (the fused tensor-core form): the host L-BFGS
+        serves it."""
+        K = self.K
+        obs = np.stack([r.observed.reshape(-1) for r in reqs])
+        rc, w, f, st = self._fit_call(s, obs, self.lbfgs_param.max_iterations)
+        if rc == -4:  # WDL_ERR_UNSUPPORTED
+            s.device_fit = False
+            return False
+        for i, r in enumerate(reqs):
+            if rc != 0:
+                r.status = rc
+                self._finish(s, r)
+                continue
+            if st[i] == -5:  # WDL_ERR_NONFINITE: an evaluation left the range
+                if fast:
+                    self._escalate(s, r)
+                    continue
+                r.status = -5
+                self._finish(s, r)
+                continue
+            r.result = w[i * K:(i + 1) * K].copy()
+            r.loss = float(f[i])
+            r.lbfgs_status = int(st[i])
+            r.status = lb.LBFGSERR_CANCELED if st[i] == lb.LBFGSERR_CANCELED else 0
+            self._finish(s, r)
+        return True
 
     def tick(self) -> int:
         """Admit what fits, collect the shape calls that have returned, then start
@@ -394,7 +450,9 @@ class ServingEngine:
 
     def capture_graphs(self, batch_headroom: int = 2):
         """Record each resident shape's one-request projection and barycenter
-        calls as CUDA graphs before serving.  A context replays a call whose
+        calls as CUDA graphs before serving (a projection's recorded call is the
+        device fit's round where the shape has one, the host L-BFGS's
+        evaluation otherwise).  A context replays a call whose
         sizes, buffers and stream it has seen twice (the first runs eagerly,
         the second is captured); those first two runs are ~1000 separate
         launches each, which a request loop on many shapes would otherwise pay
@@ -406,7 +464,16 @@ class ServingEngine:
             ctx, N = s.kernel.ctx, s.kernel.N
             atoms = f64(s.atoms)
             obs1 = f64(s.atoms.reshape(K, N)[0])
-            for P in (batch_headroom, 1, 1):
+            if self.device_fit and s.device_fit:
+                # the device fit's round (its graph does not depend on the
+                # iteration limit, so two iterations record it)
+                for P in (batch_headroom, 1):
+                    rc = self._fit_call(s, np.tile(obs1, (P, 1)), 2)[0]
+                    if rc == -4:
+                        s.device_fit = False
+                        break
+                    check(rc, ctx)
+            for P in ((batch_headroom, 1, 1) if not (self.device_fit and s.device_fit) else ()):
                 lam = f64(np.full((P, K), 1.0 / K))
                 obs = f64(np.tile(obs1, P))
                 la, loss = np.empty(P * K), np.empty(P)
