@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "lbfgs_dev.cuh"
+#include "log_group.cuh"
 #include "wdl_internal.cuh"
 
 namespace wdl {
@@ -45,8 +46,6 @@ inline int size_class(int W, int H) {
 }
 constexpr int kLfMaxK = 16;
 constexpr float kLog2e = 1.4426950408889634f;
-constexpr float kLn2 = 0.6931471805599453f;
-constexpr float kTailBits = 40.f;
 constexpr float kFloorF = -3.402823466e38f;
 
 struct LogFitProblem {
@@ -65,12 +64,6 @@ struct LogFitProblem {
   LbState* st;
   int* flag;             // 1 while the fit needs another evaluation
 };
-
-__device__ __forceinline__ float ex2f(float x) {
-  float y;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
 
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
@@ -97,23 +90,37 @@ __device__ double block_sum_d(double v, double* sh) {
 // One separable log-sum-exp axis pass of one image ([R][C] -> [C][R]), the
 // rows shared among the group: out[c][r] = log sum_k s_k exp(-(c-k)^2/gamma +
 // in[r][k]) (signs optional, in and out sign arrays distinct), as the
-// CUDA-core operator's pass but with the maximum and the sum in one pass.
+// CUDA-core operator's pass: rows staged with a halo, four neighbouring outputs
+// of a row per thread in one running-maximum pass (log_group.cuh).
 template <bool SIGNED, int G, int LR>
 __device__ void lse_pass(const float* __restrict__ in, float* __restrict__ out, int R, int C, float gamma,
                          const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign, float* sm,
                          int rank) {
-  const int CP = C + 1, SP = C + 4;
+  using namespace lse;
+  const int CP = log_cp(C), SP = log_sp(C);
   float* rows = sm;
   float* lk = rows + LR * CP;
   float* xmax = lk + C;
   uint8_t* sg = reinterpret_cast<uint8_t*>(xmax + LR);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G4 = (C + 3) >> 2;
+  const bool full = (C & 3) == 0;
   __syncthreads();
   for (int d = tid; d < C; d += kLfThreads) lk[d] = -float(d) * float(d) / gamma * kLog2e;
   for (int rb = rank; rb * LR < R; rb += G) {
     const int r0 = rb * LR, nr = min(LR, R - r0);
     __syncthreads();
     for (int rr = warp; rr < LR; rr += kLfThreads / 32) {
+      float* rw = rows + rr * CP + kHalo;
+      uint8_t* sw = sg + rr * SP + kHalo;
+      for (int k = lane; k < kHalo; k += 32) {
+        rw[-kHalo + k] = LogOps<float>::kNone;
+        rw[C + k] = LogOps<float>::kNone;
+        if (SIGNED) {
+          sw[-kHalo + k] = 1;
+          sw[C + k] = 1;
+        }
+      }
       float vm = kFloorF;
       for (int k = lane; k < C; k += 32) {
         float v = kFloorF;
@@ -122,64 +129,29 @@ __device__ void lse_pass(const float* __restrict__ in, float* __restrict__ out, 
           v = in[(size_t)(r0 + rr) * C + k] * kLog2e;
           if (SIGNED) sv = in_sign[(size_t)(r0 + rr) * C + k];
         }
-        rows[rr * CP + k] = v;
-        if (SIGNED) sg[rr * SP + k] = sv;
-        vm = v > vm ? v : vm;
+        rw[k] = v;
+        if (SIGNED) sw[k] = sv;
+        vm = fmaxf(vm, v);
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        const float w = __shfl_xor_sync(0xffffffffu, vm, o);
-        vm = w > vm ? w : vm;
-      }
+      for (int o = 16; o > 0; o >>= 1) vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
       if (lane == 0) xmax[rr] = vm;
     }
     __syncthreads();
-    for (int e = tid; e < LR * C; e += kLfThreads) {
-      const int c = e / LR, rr = e - c * LR;
+    for (int e = tid; e < LR * G4; e += kLfThreads) {
+      const int gi = e / LR, rr = e - gi * LR;
       if (rr >= nr) continue;
-      const float* row = rows + rr * CP;
-      const float X = xmax[rr];
-      const int dboth = min(c, C - 1 - c);
-      const int side = c < C - 1 - c ? 1 : -1;
-      // ONE pass: a running maximum and the sum scaled to it (a tap above the
-      // maximum rescales the sum).  Measured faster than the operator's
-      // maximum-then-sum passes on these fits (30.7 vs 25.7 problems/s on
-      // the uneven workload), slower on the 256x256 log-domain configuration,
-      // which keeps the two passes; the results agree to rounding.
-      const uint8_t* sgn = sg + rr * SP;
-      const float xc = row[c];
-      float m = xc > kFloorF ? xc : kFloorF;
-      float sum = ex2f(xc - m);
-      if (SIGNED && !sgn[c]) sum = -sum;
-      auto add = [&](float t, bool pos) {
-        if (t > m) {
-          sum = sum * ex2f(m - t) + (pos ? 1.f : -1.f);
-          m = t;
-        } else {
-          const float e = ex2f(t - m);
-          sum += pos ? e : -e;
-        }
-      };
-      int d = 1;
-      for (; d <= dboth; ++d) {
-        const float l = lk[d];
-        if (l + X < m - kTailBits) break;
-        add(l + row[c - d], !SIGNED || sgn[c - d]);
-        add(l + row[c + d], !SIGNED || sgn[c + d]);
-      }
-      if (d > dboth) {
-        for (; d < C && (side > 0 ? c + d < C : c - d >= 0); ++d) {
-          const float l = lk[d];
-          if (l + X < m - kTailBits) break;
-          const int k = c + side * d;
-          add(l + row[k], !SIGNED || sgn[k]);
-        }
-      }
-      const size_t o = (size_t)c * R + (r0 + rr);
-      if (SIGNED) {
-        out_sign[o] = sum >= 0.f ? 1 : 0;
-        out[o] = (log2f(fabsf(sum)) + m) * kLn2;
-      } else {
-        out[o] = (log2f(sum) + m) * kLn2;
+      const int c0 = 4 * gi;
+      const float* row = rows + rr * CP + kHalo;
+      const uint8_t* sgn = sg + rr * SP + kHalo;
+      float v[4];
+      bool pos[4];
+      if (full) log_group<float, SIGNED, true>(row, sgn, lk, xmax[rr], c0, C, v, pos);
+      else log_group<float, SIGNED, false>(row, sgn, lk, xmax[rr], c0, C, v, pos);
+      const int nv = min(4, C - c0);
+      for (int j = 0; j < nv; ++j) {
+        const size_t o = (size_t)(c0 + j) * R + (r0 + rr);
+        out[o] = v[j];
+        if (SIGNED) out_sign[o] = pos[j] ? 1 : 0;
       }
     }
   }
@@ -331,7 +303,7 @@ __global__ void __launch_bounds__(kLfThreads)
 inline size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
 size_t lse_smem(int C, int LR) {
-  return ((size_t)LR * (C + 1) + C + LR) * sizeof(float) + (size_t)LR * (C + 4) + 16;
+  return ((size_t)LR * lse::log_cp(C) + C + LR) * sizeof(float) + (size_t)LR * lse::log_sp(C) + 16;
 }
 
 template <int G, int LR>
