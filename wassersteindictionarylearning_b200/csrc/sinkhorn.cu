@@ -327,19 +327,29 @@ __global__ void k_bwd_pre(const T* __restrict__ n, const T* __restrict__ v,
 }
 
 // gradDic += c / cb[s-1]; tmp = -p c / cb^2 (dictionary recursion, when it
-// runs); convu *= -p / cb^2 (:612-617, :655-660).
+// runs); convu *= -p / cb^2 (:612-617, :655-660).  Thread per dictionary
+// entry q = (k, j), histograms p in order: the dictionary gradient gdic[q] (KN
+// doubles, summed over p here rather than kept per histogram) takes this
+// round's sum over p in one update.
 template <typename T>
 __global__ void k_bwd_mid(const T* __restrict__ c, const T* __restrict__ cb,
                           const T* __restrict__ atoms, double* __restrict__ gdic,
-                          T* __restrict__ nxt, size_t KN, size_t PKN, int weights, int dict) {
-  GRID_STRIDE(i, PKN) {
-    const T cbv = cb[i], pa = atoms[i % KN];
-    if (dict) {
-      const T cc = c[i];
-      gdic[i] += (double)(cc / cbv);
-      nxt[i] = -pa * cc / (cbv * cbv);
+                          T* __restrict__ nxt, size_t KN, int P, size_t PKN, int weights, int dict) {
+  GRID_STRIDE(q, KN) {
+    const T pa = atoms[q];
+    double g = 0;
+#pragma unroll 4
+    for (int p = 0; p < P; ++p) {
+      const size_t i = (size_t)p * KN + q;
+      const T cbv = cb[i];
+      if (dict) {
+        const T cc = c[i];
+        g += (double)(cc / cbv);
+        nxt[i] = -pa * cc / (cbv * cbv);
+      }
+      if (weights) nxt[PKN + i] = c[PKN + i] * (-pa / (cbv * cbv));
     }
-    if (weights) nxt[PKN + i] = c[PKN + i] * (-pa / (cbv * cbv));
+    if (dict) gdic[q] += g;
   }
 }
 
@@ -367,6 +377,95 @@ __global__ void k_bwd_post(const T* __restrict__ c2, const T* __restrict__ phi_p
     if (dict) n[idx] = sn;
     gw[idx] = sg;
   }
+}
+
+// Round s's k_bwd_post followed by round s-1's k_bwd_pre in one pass (the
+// kernel-domain counterpart of k_lbwd_post_pre below): v, r, n and gw never go
+// to memory.  Block per (p, segment), one warp per atom (blockDim 32 K, K <=
+// 32), two 32-pixel chunks per round, the next round's loads issued before
+// this round's sums; n and gw are summed over the atoms in k order through
+// SMEM (as k_bwd_post), the dot partial of (p, k) over the segment is the
+// lanes' sums reduced across the warp (an order fixed by N).  dict: the
+// dictionary recursion runs (v, n, tmp).
+template <typename T>
+struct BwdIn {
+  T cv[2], cr[2], ph[2], bp[2];
+};
+
+template <typename T>
+__device__ __forceinline__ void bwd_load(BwdIn<T>& in, const T* __restrict__ c2, const T* __restrict__ phi_p,
+                                         const T* __restrict__ b_p, size_t ib, size_t jb, size_t j1, int jj,
+                                         size_t PKN, int dict) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const size_t j = jb + 32 * h + jj;
+    in.cv[h] = in.cr[h] = T(0);
+    in.ph[h] = in.bp[h] = T(1);
+    if (j < j1) {
+      const size_t i = ib + j;
+      if (dict) in.cv[h] = c2[i];
+      in.cr[h] = c2[PKN + i];
+      in.ph[h] = phi_p[i];
+      in.bp[h] = b_p[i];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_bwd_post_pre(
+    const T* __restrict__ c2, const T* __restrict__ phi_p, const T* __restrict__ b_p,
+    const T* __restrict__ lam, T* __restrict__ tmp, T* __restrict__ u, double* __restrict__ part, int K,
+    size_t N, size_t PKN, int dict) {
+  constexpr int W = 64;  // pixels per round
+  extern __shared__ __align__(16) unsigned char bwd_raw[];
+  T* vs = reinterpret_cast<T*>(bwd_raw);  // [K][W]
+  T* rs = vs + K * W;                     // [K][W]
+  T* sums = rs + K * W;                   // [2][W]: n, gw
+  const int k = threadIdx.x >> 5, jj = threadIdx.x & 31;
+  const size_t p = blockIdx.x;
+  const size_t j0 = (size_t)blockIdx.y * kSegElems, j1 = min(N, j0 + kSegElems);
+  const T l = lam[p * K + k];
+  const size_t ib = (p * K + k) * N;
+  double acc = 0;
+  BwdIn<T> cur, nxt;
+  bwd_load(cur, c2, phi_p, b_p, ib, j0, j1, jj, PKN, dict);
+  for (size_t jb = j0; jb < j1; jb += W) {
+    T vv[2], rr[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      vv[h] = dict ? cur.cv[h] / cur.ph[h] : T(0);
+      rr[h] = cur.cr[h] * cur.bp[h];
+      if (jb + 32 * h + jj >= j1) vv[h] = rr[h] = T(0);
+      vs[k * W + 32 * h + jj] = vv[h];
+      rs[k * W + 32 * h + jj] = rr[h];
+    }
+    __syncthreads();
+    if (jb + W < j1) bwd_load(nxt, c2, phi_p, b_p, ib, jb + W, j1, jj, PKN, dict);
+    for (int q = threadIdx.x; q < 2 * W; q += blockDim.x) {
+      if (!dict && q < W) continue;
+      const T* src = q < W ? vs + q : rs + (q - W);
+      T a = T(0);
+      for (int kk = 0; kk < K; ++kk) a += src[kk * W];
+      sums[q] = a;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t j = jb + 32 * h + jj;
+      if (j < j1) {
+        const size_t i = ib + j;
+        const T sg = sums[W + 32 * h + jj];
+        if (dict) tmp[i] = (l * sums[32 * h + jj] - vv[h]) * cur.bp[h];
+        acc += acc_log<T>(cur.ph[h]) * (double)sg;
+        u[i] = (l * sg - rr[h]) / cur.ph[h];
+      }
+    }
+    __syncthreads();
+    cur = nxt;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (jj == 0) part[(p * K + k) * gridDim.y + blockIdx.y] = acc;
 }
 
 // ---------------- log-domain reverse pass (:722-812), one round s -------------------
@@ -557,15 +656,6 @@ __global__ void __launch_bounds__(1024) k_lbwd_post_pre(
 }
 
 // ---------------- reductions and evaluate_both epilogue (:1086-1136) ----------------
-__global__ void k_sum_over_p(const double* __restrict__ gdic, double* __restrict__ out, int P,
-                             size_t KN) {
-  GRID_STRIDE(i, KN) {
-    double s = 0;
-    for (int p = 0; p < P; ++p) s += gdic[(size_t)p * KN + i];
-    out[i] = s;
-  }
-}
-
 // Weight part of g: (la - <w, la>) * w / scale (projection :1093-1098, chain rule
 // :1125-1128, scaling :1135-1136).  One histogram per thread.
 __global__ void k_project_weights(const double* __restrict__ la, const double* __restrict__ w,
@@ -799,8 +889,8 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
   const int dict = (result_dic || log_domain) ? 1 : 0;
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.v, 0, PKN * sizeof(T), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.r, 0, PKN * sizeof(T), s));
-  // the log domain sums the dictionary gradient over p as it goes (KN entries)
-  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, (log_domain ? KN : PKN) * sizeof(double), s));
+  // the dictionary gradient is summed over p as it goes (KN entries)
+  WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.gdic, 0, KN * sizeof(double), s));
   WDL_CUDA_TRY(ctx, cudaMemsetAsync(B.dot, 0, (size_t)P * K * sizeof(double), s));
   T* tmp = B.buf2;
   T* u = B.buf2 + PKN;
@@ -811,9 +901,12 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
     const bool more = sstep > 1;
     const size_t nimg = (size_t)(more ? 2 : 1) * P * K;
     if (!log_domain) {
-      k_bwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
-          B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dpart, K, N, dict);
-      WDL_LAUNCH_CHECK(ctx);
+      // the first round's pre here; later rounds' pre ran with the previous post
+      if (sstep == L || K > kFuseK) {
+        k_bwd_pre<T><<<dim3((unsigned)(P * K), (unsigned)n_segments(N)), 256, 0, s>>>(
+            B.n, B.v, b_s, B.gw, B.r, phi_s, B.lam, tmp, u, B.dpart, K, N, dict);
+        WDL_LAUNCH_CHECK(ctx);
+      }
       k_add_partials<<<(P * K + 127) / 128, 128, 0, s>>>(B.dot, B.dpart, P * K, (int)n_segments(N));
       WDL_LAUNCH_CHECK(ctx);
       if (dict) {
@@ -822,7 +915,8 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
         if ((rc = conv_stack<T>(ctx, u, B.cbuf2 + PKN, B.ctmp, (size_t)P * K, s))) return rc;
       }
       if (dict || more) {
-        k_bwd_mid<T><<<G_PKN, 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, PKN, more, dict);
+        k_bwd_mid<T><<<launch_cfg(ctx, KN), 256, 0, s>>>(B.cbuf2, cb_p, B.atoms, B.gdic, B.buf2, KN, P, PKN,
+                                                       more, dict);
         WDL_LAUNCH_CHECK(ctx);
       }
       if (!more) break;
@@ -833,7 +927,13 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
       }
       const T* phi_p = B.tape_phi + (size_t)(sstep - 2) * PKN;
       const T* b_p = B.tape_b + (size_t)(sstep - 1) * PKN;
-      k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN, dict);
+      if (K <= kFuseK) {
+        k_bwd_post_pre<T><<<dim3((unsigned)P, (unsigned)n_segments(N)), 32 * K,
+                            (size_t)(2 * K + 2) * 64 * sizeof(T), s>>>(B.cbuf2, phi_p, b_p, B.lam, tmp, u,
+                                                                       B.dpart, K, N, PKN, dict);
+      } else {
+        k_bwd_post<T><<<G_PN, 256, 0, s>>>(B.cbuf2, phi_p, b_p, B.v, B.r, B.n, B.gw, K, N, PN, PKN, dict);
+      }
       WDL_LAUNCH_CHECK(ctx);
     } else {
       // the first round's pre here; later rounds' pre ran with the previous post
@@ -871,12 +971,8 @@ int gradient_both_t(wdl_ctx* ctx, int P, int K, int L, int loss_type, const doub
 
   // Outputs.
   WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_la, B.dot, (size_t)P * K * 8, cudaMemcpyDeviceToDevice, s));
-  if (result_dic && log_domain) {
+  if (result_dic)
     WDL_CUDA_TRY(ctx, cudaMemcpyAsync(result_dic, B.gdic, KN * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  } else if (result_dic) {
-    k_sum_over_p<<<launch_cfg(ctx, KN), 256, 0, s>>>(B.gdic, result_dic, P, KN);
-    WDL_LAUNCH_CHECK(ctx);
-  }
   if (bary_out) {
     k_cast_back<T><<<G_PN, 256, 0, s>>>(B.bary, bary_out, PN);
     WDL_LAUNCH_CHECK(ctx);
