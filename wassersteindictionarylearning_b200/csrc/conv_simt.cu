@@ -222,7 +222,7 @@ __device__ __forceinline__ void log_stage(const T* __restrict__ in, const uint8_
 // SQ > 0: the images are SQ x SQ (R = C = SQ), known at compile time, so
 // strides and loop bounds are constants.
 template <typename T, bool SIGNED, int LR, bool SUB, int SQ>
-__global__ void __launch_bounds__(256, SIGNED ? 4 : 5) log_axis_pass_kernel(
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (SIGNED ? 4 : 5) : 2) log_axis_pass_kernel(
     const T* __restrict__ in, T* __restrict__ out, int R_, int C_, size_t img_stride, T gamma_t,
     const uint8_t* __restrict__ in_sign, uint8_t* __restrict__ out_sign,
     unsigned long long* __restrict__ exps, const T* __restrict__ sub_from, T* __restrict__ sub_out,
